@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""CCD step benchmark (update + traverse + ACCD) on the 2.1M-triangle cloth.
+
+Workload: 1025 x 1025 wavy cloth (2,097,152 triangles, float64 V, int32 F,
+thickness 1e-4), seeded synthetic data.  One step = BVHTree::update(V0, V1,
+F) + traverse(V0, V1, F) through the C ABI; F never changes, so every timed
+step takes the refit-only path, and V1 alternates between two seeded draws.
+The first (full LBVH build) update is timed separately.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  value = candidate stencils / second of the
+whole job with inputs resident in HBM; e2e = the same through the C ABI from
+pinned host buffers, host<->device copies of inputs and of every hit and
+discrete pair inside the timed region.  --impl reference times the
+reference's own CPU code (the oracle build of the unmodified reference
+sources) on the host cores, on a 257-row strip of the same cloth per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CCD step ms & stencils/s at 2.1M tris: FP32-certified vs FP64 GPU vs TBB"
+UNIT = "stencils/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=1025, help="cloth grid side")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32cert"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# Algorithmic work per unit (also stated in DESIGN.md).
+#   walk   : per query leaf its FP64 box (96 B) + prim id (4) + active (1), the
+#            n-1 internal nodes once (64 B), and per leaf pair found the
+#            candidate leaf box (96 B) + its prim id (4) + the pair write (8).
+#   expand : per leaf pair 8 B read + 2 x (12 B face + 1 B flags) + 16 B per
+#            stencil written + 8 B per discrete pair, + the tri-tri gather of
+#            6 V1 vertices (144 B) per pair.
+#   narrow : per stencil 16 B read + 2 x 4 x 24 B vertex gather (192 B), plus
+#            25 B per hit written (int4 stencil, f64 toi, u8 kind).
+#   refit  : per leaf 12 B face + 6 x 24 B vertex reads, 96 B FP64 box + 1 B
+#            active written, 32 B of node slot written, 64 B per internal node read.
+def algorithmic_bytes(c, n):
+    walk = n * (96 + 4 + 1) + (n - 1) * 64 + c["leaf_pairs"] * (96 + 4 + 8)
+    expand = c["leaf_pairs"] * (8 + 26 + 144) + 16 * (c["vf"] + c["ee"]) + 8 * c["discrete"]
+    narrow = (c["vf"] + c["ee"]) * (16 + 192) + 25 * c["hits"]
+    refit = n * (12 + 144 + 96 + 1 + 32) + (n - 1) * 64
+    return {"walk": walk, "expand": expand, "narrow": narrow, "refit": refit}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from mclccd_b200 import scenes
+    from oracle.ref import REF_SO, Port, Reference
+    rows = 257
+    V0, V1a, F, eta = scenes.wavy_cloth(args.n, seed=0, rows=rows)
+    V1b = scenes.wavy_redraw(V0, 1)
+    if os.path.exists(REF_SO):
+        R, kind = Reference(), "reference"
+        rec = R.run(V0, V1b, F, eta)
+        n_sten = len(rec["cand_sten"])
+        cores = R.L.ref_threads()
+    else:
+        R, kind = None, "port"
+        p = Port().run(V0, V1b, F, eta)
+        n_sten = len(p["cand_sten"])
+        cores = 1
+    times = []
+    for it in range(args.warmup + args.steps):
+        if R is not None:
+            r = R.time(V0, V1a, F, eta, V1b=V1b)
+            ms = r["ms_update_again"] + r["ms_traverse"]
+        else:
+            t0 = time.perf_counter()
+            Port().run(V0, V1b, F, eta)
+            ms = (time.perf_counter() - t0) * 1e3
+        if it >= args.warmup:
+            times.append(ms)
+    ms = float(np.mean(times))
+    val = n_sten / (ms / 1e3)
+    sample = (f"{rows}-row strip of the {args.n}x{args.n} wavy cloth ({len(F)} tris, {n_sten} stencils): "
+              f"update + traverse per step")
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"wavy cloth {args.n}x{args.n} (2,097,152 tris), thickness 1e-4; "
+                                   f"reference steps on a {rows}-row strip", "tris_per_step": int(len(F)),
+                       "stencils_per_step": int(n_sten)},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline(V0, V1a, V1b, F, eta, n_sten):
+    from oracle.ref import REF_SO, Reference
+    if not os.path.exists(REF_SO):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "reference build missing"}
+    R = Reference()
+    r = R.time(V0, V1a, F, eta, V1b=V1b)
+    ms = r["ms_update_again"] + r["ms_traverse"]
+    return {"value": n_sten / (ms / 1e3), "unit": UNIT, "cores": r["threads"], "kind": "reference",
+            "sample": (f"one full step of the same workload ({len(F)} tris): second update (same F) "
+                       f"{r['ms_update_again']:.0f} ms + traverse {r['ms_traverse']:.0f} ms; first update "
+                       f"{r['ms_update_first']:.0f} ms"),
+            "ms_per_step": ms}
+
+
+def run_b200(args, rank, world, local):
+    import torch
+    from mclccd_b200 import MEM_HOST, PREC_FP32_CERTIFIED, PREC_FP64, BVHTree, scenes
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    V0, V1a, F, eta = scenes.wavy_cloth(args.n, seed=0)
+    V1b = scenes.wavy_redraw(V0, 1)
+    n = len(F)
+    dev = torch.device("cuda", local)
+    dV0, dV1a, dV1b, dF = (torch.from_numpy(a).to(dev) for a in (V0, V1a, V1b, F))
+    stream = torch.cuda.current_stream()
+    prec = PREC_FP32_CERTIFIED if args.precision == "fp32cert" else PREC_FP64
+    tree = BVHTree(3, precision=prec)
+    tree.options.box_eta = tree.options.vf_ccd_eta = tree.options.ee_ccd_eta = eta
+    tree.options.profile = True
+    tree.set_stream(stream.cuda_stream)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    # first update: full build (representative flags, Morton, sort, hierarchy, refit)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    tree.update(dV0, dV1a, dF)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    first_ms = e0.elapsed_time(e1)
+    tree.traverse()
+    V1s = [dV1b, dV1a]
+    for i in range(args.warmup):
+        tree.update(dV0, V1s[i % 2], dF)
+        tree.traverse()
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = tree.kernel_launches()
+    step_ms, sten, stages = [], 0, []
+    clocks.start()
+    for i in range(args.steps):
+        flush.zero_()                        # evict L2 between timed steps (outside the events)
+        s0, s1 = ev(), ev()
+        s0.record(stream)
+        tree.update(dV0, V1s[i % 2], dF)
+        tree.traverse()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(s0.elapsed_time(s1))
+        c = tree.counts()
+        sten += c["vf"] + c["ee"]
+        stages.append(tree.stage_ms())
+    clk = clocks.stop()
+    launches = tree.kernel_launches() - launches0
+    total_s = sum(step_ms) / 1e3
+    if dist:
+        t = torch.tensor([total_s, float(sten)], dtype=torch.float64, device=dev)
+        tmax = t.clone(); dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone(); dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        total_max, sten_all = float(tmax[0]), float(tsum[1])
+    else:
+        total_max, sten_all = total_s, float(sten)
+    value = sten_all / total_max
+    c = tree.counts()
+    stage = {k: float(np.median([s[k] for s in stages])) for k in stages[0]}
+
+    # roofline of the dominant kernel: algorithmic bytes / its device time
+    ab = algorithmic_bytes(c, n)
+    kt = {"walk": stage["walk"], "expand": stage["expand"], "narrow": stage["narrow"], "refit": stage["refit"]}
+    top = max(kt, key=kt.get)
+    peak, src = measured_peaks()
+    achieved = ab[top] / (kt[top] / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_source": src,
+            "algorithmic_bytes": ab[top], "kernel_ms": kt[top],
+            "all": {k: {"ms": kt[k], "GB/s": ab[k] / (kt[k] / 1e3) / 1e9 if kt[k] > 0 else None} for k in kt}}
+
+    # end to end through the C ABI from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(a).pin_memory()
+        hV0, hV1a, hV1b, hF = pin(V0), pin(V1a), pin(V1b), pin(F)
+        cap = int(c["hits"] * 1.5) + 1024
+        hs = torch.empty((cap, 4), dtype=torch.int32).pin_memory()
+        hv = torch.empty(cap, dtype=torch.uint8).pin_memory()
+        ht = torch.empty(cap, dtype=torch.float64).pin_memory()
+        hd = torch.empty((max(1024, int(c["discrete"] * 1.5)), 2), dtype=torch.int32).pin_memory()
+        L = tree._L
+        hV1s = [hV1b, hV1a]
+        e_ms, h2d, d2h = [], 0, 0
+        for i in range(args.warmup + args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s0, s1 = ev(), ev()
+            s0.record(stream)
+            tree.update(hV0.numpy(), hV1s[i % 2].numpy(), hF.numpy())
+            tree.traverse()
+            cc = tree.counts()
+            L.mclccd_get_hits(tree._h, MEM_HOST, cap, hs.data_ptr(), hv.data_ptr(), ht.data_ptr())
+            L.mclccd_get_discrete(tree._h, MEM_HOST, hd.shape[0], hd.data_ptr())
+            s1.record(stream)
+            torch.cuda.synchronize()
+            wall = (time.perf_counter() - t0) * 1e3
+            if i >= args.warmup:
+                e_ms.append(max(s0.elapsed_time(s1), wall))
+                h2d = V0.nbytes + V1a.nbytes + F.nbytes
+                d2h = cc["hits"] * (16 + 1 + 8) + cc["discrete"] * 8
+        e_total = sum(e_ms) / 1e3
+        if dist:
+            t = torch.tensor([e_total], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_total = float(t[0])
+        e2e = {"value": sten_all / e_total * (1.0 if True else 0), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": e_total * 1e3 / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(V0, V1a, V1b, F, eta, c["vf"] + c["ee"])
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_max * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == PREC_FP64 else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": f"wavy cloth {args.n}x{args.n} ({n} tris), thickness 1e-4, refit-only "
+                                   "update + traverse + ACCD per step (F unchanged, V1 alternates two seeded draws)",
+                       "tris": n, "stencils_per_step": int(c["vf"] + c["ee"]), "vf": int(c["vf"]),
+                       "ee": int(c["ee"]), "hits": int(c["hits"]), "discrete": int(c["discrete"]),
+                       "leaf_pairs": int(c["leaf_pairs"]), "first_update_ms": first_ms,
+                       "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "flushed between timed steps (512 MB write outside the timed events)",
+                       "stage_ms_median": stage, "step_ms_all": step_ms},
+            "gpu_launches": int(launches), "roofline": roof, "clocks": clk}
+    if e2e is not None:
+        line["e2e"] = e2e
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_b200(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

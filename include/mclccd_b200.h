@@ -1,0 +1,150 @@
+/*
+ * mclccd_b200 -- C ABI of the B200 continuous-collision-detection path.
+ *
+ * Drop-in for the hot path of mattoverby/mclccd's mcl::BVHTree<double,DIM>
+ * (include/MCL/BVHTree.hpp): update(V0,V1,P) builds the hierarchy over swept
+ * primitive boxes, traverse(V0,V1,P) finds every candidate vertex-face /
+ * edge-edge stencil, runs the ACCD narrow phase and the discrete test, and
+ * leaves the results (what the reference hands to append_pair and
+ * append_discrete) in device buffers that the get_* calls copy out.
+ *
+ * Conventions
+ *   - Positions are float64, row-major nv x dim; primitives int32, row-major
+ *     np x pdim (triangles in 3D, edges in 2D).
+ *   - mem_kind says where the caller's arrays live (MCLCCD_MEM_HOST or
+ *     MCLCCD_MEM_DEVICE, device = the current CUDA device's global memory).
+ *   - Every call returns a status (MCLCCD_OK == 0).  The reference has no
+ *     error codes (asserts and silent early returns); here bad input is an
+ *     error instead of undefined behaviour.
+ *   - A handle is not thread-safe; all its work is ordered on its stream.
+ *   - Stencils are int32[4]: VF = [v, f0, f1, f2] (2D: [v, e0, e1, -1]),
+ *     EE = [a, b, c, d] (edge a-b of the lower-indexed triangle first).
+ *     Discrete pairs are (p0, p1) with p0 < p1.
+ */
+#ifndef MCLCCD_B200_H
+#define MCLCCD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mclccd_tree mclccd_tree;
+
+/* Status codes. */
+#define MCLCCD_OK 0
+#define MCLCCD_ERR_INVALID 1     /* bad argument or primitive index out of [0, nv) */
+#define MCLCCD_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define MCLCCD_ERR_NOMEM 3       /* device allocation failed */
+#define MCLCCD_ERR_OVERFLOW 4    /* caller's output capacity too small (copied a prefix) */
+#define MCLCCD_ERR_STATE 5       /* traverse before update, or results before traverse */
+#define MCLCCD_ERR_DEVICE 6      /* a kernel gave up a bounded wait or overflowed its stack */
+#define MCLCCD_ERR_UNSUPPORTED 7 /* option not provided by this path (vf_one_sided) */
+
+/* Where caller arrays live. */
+#define MCLCCD_MEM_HOST 0
+#define MCLCCD_MEM_DEVICE 1
+
+/* Option flags: the booleans of BVHTree::Options (BVHTree.hpp:42-64). */
+#define MCLCCD_OPT_REPTRI (1u << 0)
+#define MCLCCD_OPT_THREADED (1u << 1)     /* accepted; the device path is always parallel */
+#define MCLCCD_OPT_DISCRETE (1u << 2)
+#define MCLCCD_OPT_CONTINUOUS (1u << 3)
+#define MCLCCD_OPT_VF_ONE_SIDED (1u << 4) /* CTCD narrow phase: not provided (UNSUPPORTED) */
+#define MCLCCD_OPT_EE_ROBUST (1u << 5)    /* accepted; unused by ACCD, as in the reference */
+#define MCLCCD_OPT_DEFAULT (MCLCCD_OPT_REPTRI | MCLCCD_OPT_THREADED | MCLCCD_OPT_DISCRETE | \
+                            MCLCCD_OPT_CONTINUOUS | MCLCCD_OPT_EE_ROBUST)
+/* Extra behaviour flags (not in the reference). */
+#define MCLCCD_OPT_ALWAYS_REBUILD (1u << 8) /* never take the refit-only path */
+#define MCLCCD_OPT_PROFILE (1u << 9)        /* record per-stage CUDA-event times */
+
+/* Narrow-phase precision. */
+#define MCLCCD_PREC_FP64 0
+#define MCLCCD_PREC_FP32_CERTIFIED 1
+
+/* Replaces: BVHTree<double,DIM>::BVHTree() (BVHTree.cpp:20-24).  dim is 2 or
+ * 3; the tree lives on the current CUDA device and gets its own stream.
+ * Options start at the reference defaults (BVHTree.hpp:52-62). */
+int mclccd_create(int dim, mclccd_tree **out);
+
+/* Replaces: ~BVHTree().  Frees every device buffer the handle owns. */
+int mclccd_destroy(mclccd_tree *tree);
+
+/* Replaces: writes to BVHTree::options (BVHTree.hpp:42-64). */
+int mclccd_set_options(mclccd_tree *tree, double box_eta, double vf_ccd_eta, double ee_ccd_eta, unsigned flags);
+/* Reads them back (update() clamps the two gaps to box_eta, BVHTree.cpp:39-40). */
+int mclccd_get_options(const mclccd_tree *tree, double *box_eta, double *vf_ccd_eta, double *ee_ccd_eta,
+                       unsigned *flags);
+
+/* Orders all of the handle's work on a caller stream (cudaStream_t; NULL
+ * restores the handle's own stream). */
+int mclccd_set_stream(mclccd_tree *tree, void *stream);
+
+/* MCLCCD_PREC_FP64 (default; bit-exact with the reference) or
+ * MCLCCD_PREC_FP32_CERTIFIED (FP32 filter + FP64 certification). */
+int mclccd_set_precision(mclccd_tree *tree, int precision);
+
+/* Replaces: BVHTree::update(const T*V0, const T*V1, const int*P, int np,
+ * int pdim, const int*active) (BVHTree.hpp:81-82, BVHTree.cpp:27-126).
+ * nv is new: the device needs the vertex count to copy/validate V0, V1.
+ * active is an optional per-vertex int mask (NULL = all active).  When np,
+ * pdim, nv and the bytes of P equal the previous update, only the boxes are
+ * refitted; otherwise the hierarchy is rebuilt.  np == 0 clears the tree. */
+int mclccd_update(mclccd_tree *tree, const double *V0, const double *V1, int nv, const int *P, int np, int pdim,
+                  const int *active, int mem_kind);
+
+/* Replaces: BVHTree::traverse(const T*V0, const T*V1, const int*P) const
+ * (BVHTree.hpp:86, BVHTree.cpp:129-159) with the default narrow phase and no
+ * filter.  Passing V0 = V1 = P = NULL reuses the arrays of the last update.
+ * Results stay on the device until read with mclccd_get_*. */
+int mclccd_traverse(mclccd_tree *tree, const double *V0, const double *V1, int nv, const int *P, int mem_kind);
+
+/* Counts from the last traverse: CCD hits (append_pair calls), discrete
+ * pairs (append_discrete calls), candidate VF / EE stencils (filter_pair
+ * calls) and leaf pairs whose boxes intersect.  Any pointer may be NULL. */
+int mclccd_counts(const mclccd_tree *tree, long long *n_hits, long long *n_discrete, long long *n_vf,
+                  long long *n_ee, long long *n_leaf_pairs);
+
+/* Copies up to capacity hits: sten int32[4*n], is_vf uint8[n], toi f64[n]
+ * (any of them may be NULL).  The arguments of append_pair (BVHTree.hpp:102). */
+int mclccd_get_hits(mclccd_tree *tree, int mem_kind, long long capacity, int *sten, unsigned char *is_vf,
+                    double *toi);
+
+/* Copies up to capacity discrete pairs int32[2*n], p0 < p1.  The arguments of
+ * append_discrete (BVHTree.hpp:108). */
+int mclccd_get_discrete(mclccd_tree *tree, int mem_kind, long long capacity, int *pairs);
+
+/* Copies up to capacity candidate stencils (every stencil the reference
+ * passes to filter_pair, BVHTree.cpp:345,368,393): VF first, then EE. */
+int mclccd_get_candidates(mclccd_tree *tree, int mem_kind, long long capacity, int *sten, unsigned char *is_vf);
+
+/* Leaf data of the last update in primitive order (BVHTree::leaves):
+ * boxes f64[np * 6 * dim] as (box.min, box.max, t0.min, t0.max, t1.min,
+ * t1.max) and flags uint8[np] (bit j: vertex slot j represented, bit 3+j:
+ * edge slot j represented, bit 6: active). */
+int mclccd_get_leaves(mclccd_tree *tree, double *boxes, unsigned char *flags);
+
+/* Bulk narrow phase (added entry point): NarrowPhaseACCD::query_ccd_vf/ee
+ * (NarrowPhase.cpp:609-631) over n caller stencils.  out_toi[i] = toi on a
+ * hit, -1 otherwise; out_hit[i] = 1/0.  stream may be NULL (default stream).
+ * All arrays are on the same side (mem_kind). */
+int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv, const int *sten,
+                             const unsigned char *is_vf, long long n, double vf_ccd_eta, double ee_ccd_eta,
+                             double *out_toi, int *out_hit, int mem_kind, void *stream);
+
+/* Per-stage device times (ms) of the last update + traverse when
+ * MCLCCD_OPT_PROFILE is set: [update_total, build, refit, traverse_total,
+ * tree_walk, expand, narrow]; returns how many were written. */
+int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
+
+/* Kernels launched by this handle since creation (for launch accounting). */
+int mclccd_kernel_launches(const mclccd_tree *tree, long long *n);
+
+/* Human-readable message of the handle's last failure ("" if none). */
+const char *mclccd_last_error(const mclccd_tree *tree);
+const char *mclccd_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCLCCD_B200_H */

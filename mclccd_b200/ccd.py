@@ -1,0 +1,312 @@
+"""Python mirror of mclccd's ``mcl::BVHTree<double, DIM>`` over the C ABI.
+
+Same members and meaning as the reference (include/MCL/BVHTree.hpp):
+``options`` (box_eta, vf_ccd_eta, ee_ccd_eta, reptri, threaded, discrete,
+continuous, vf_one_sided, ee_robust), ``update(V0, V1, P, active=None)``,
+``traverse(V0, V1, P)`` and the hooks ``append_pair(sten, is_vf, toi)`` and
+``append_discrete(p0, p1) -> stop``.  The CCD work runs on the GPU; after
+``traverse`` the results are also available as arrays (``hits()``,
+``discrete()``, ``candidates()``).
+
+``filter_pair`` and ``narrow_phase`` are honoured on the host: when set,
+``traverse`` copies the candidate stencils out, drops those ``filter_pair``
+rejects and scores the rest with ``narrow_phase`` (or the device ACCD when
+only a filter is set).  Hooks are called from the calling thread.
+
+Arrays may be numpy arrays (host) or CUDA torch tensors (device); there is
+no CPU fallback: without the built library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmclccd_b200.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_OVERFLOW, ERR_STATE, ERR_DEVICE, ERR_UNSUPPORTED = range(8)
+MEM_HOST, MEM_DEVICE = 0, 1
+OPT_REPTRI, OPT_THREADED, OPT_DISCRETE, OPT_CONTINUOUS = 1, 2, 4, 8
+OPT_VF_ONE_SIDED, OPT_EE_ROBUST = 16, 32
+OPT_ALWAYS_REBUILD, OPT_PROFILE = 1 << 8, 1 << 9
+PREC_FP64, PREC_FP32_CERTIFIED = 0, 1
+
+_lib = None
+
+
+class CCDError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"mclccd_b200 status {status}: {msg}")
+        self.status = status
+
+
+def lib():
+    """Loads libmclccd_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C mclccd_b200`")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip, ucp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_ubyte)
+    llp = C.POINTER(C.c_longlong)
+    sig = {
+        "mclccd_create": ([C.c_int, C.POINTER(vp)], C.c_int),
+        "mclccd_destroy": ([vp], C.c_int),
+        "mclccd_set_options": ([vp, C.c_double, C.c_double, C.c_double, C.c_uint], C.c_int),
+        "mclccd_get_options": ([vp, dp, dp, dp, C.POINTER(C.c_uint)], C.c_int),
+        "mclccd_set_stream": ([vp, vp], C.c_int),
+        "mclccd_set_precision": ([vp, C.c_int], C.c_int),
+        "mclccd_update": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int], C.c_int),
+        "mclccd_traverse": ([vp, vp, vp, C.c_int, vp, C.c_int], C.c_int),
+        "mclccd_counts": ([vp, llp, llp, llp, llp, llp], C.c_int),
+        "mclccd_get_hits": ([vp, C.c_int, C.c_longlong, vp, vp, vp], C.c_int),
+        "mclccd_get_discrete": ([vp, C.c_int, C.c_longlong, vp], C.c_int),
+        "mclccd_get_candidates": ([vp, C.c_int, C.c_longlong, vp, vp], C.c_int),
+        "mclccd_get_leaves": ([vp, vp, vp], C.c_int),
+        "mclccd_narrow_phase_bulk": ([C.c_int, vp, vp, C.c_int, vp, vp, C.c_longlong, C.c_double, C.c_double,
+                                      vp, vp, C.c_int, vp], C.c_int),
+        "mclccd_stage_ms": ([vp, C.POINTER(C.c_float), C.c_int], C.c_int),
+        "mclccd_kernel_launches": ([vp, llp], C.c_int),
+        "mclccd_last_error": ([vp], C.c_char_p),
+        "mclccd_status_string": ([C.c_int], C.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _is_torch_cuda(a) -> bool:
+    return type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False)
+
+
+def _arg(a, dtype, cols=None):
+    """(pointer, mem_kind, keepalive, rows) for a numpy array or CUDA tensor."""
+    if a is None:
+        return None, None, None, 0
+    if _is_torch_cuda(a):
+        import torch
+        tdt = {np.float64: torch.float64, np.int32: torch.int32, np.uint8: torch.uint8}[dtype]
+        if a.dtype != tdt:
+            raise TypeError(f"expected {tdt}, got {a.dtype}")
+        a = a.contiguous()
+        return C.c_void_p(a.data_ptr()), MEM_DEVICE, a, (a.shape[0] if a.dim() else 0)
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    if cols is not None and arr.ndim == 1:
+        arr = arr.reshape(-1, cols)
+    return C.c_void_p(arr.ctypes.data), MEM_HOST, arr, (arr.shape[0] if arr.ndim else 0)
+
+
+@dataclass
+class Options:
+    """BVHTree::Options (BVHTree.hpp:42-64) with the reference defaults."""
+    box_eta: float = 1e-6
+    vf_ccd_eta: float = 1e-6
+    ee_ccd_eta: float = 1e-6
+    reptri: bool = True
+    threaded: bool = True
+    discrete: bool = True
+    continuous: bool = True
+    vf_one_sided: bool = False
+    ee_robust: bool = True
+    always_rebuild: bool = False
+    profile: bool = False
+
+    def flags(self) -> int:
+        f = 0
+        for name, bit in (("reptri", OPT_REPTRI), ("threaded", OPT_THREADED), ("discrete", OPT_DISCRETE),
+                          ("continuous", OPT_CONTINUOUS), ("vf_one_sided", OPT_VF_ONE_SIDED),
+                          ("ee_robust", OPT_EE_ROBUST), ("always_rebuild", OPT_ALWAYS_REBUILD),
+                          ("profile", OPT_PROFILE)):
+            if getattr(self, name):
+                f |= bit
+        return f
+
+
+class BVHTree:
+    """mcl::BVHTree<double, dim> on the GPU."""
+
+    def __init__(self, dim: int = 3, precision: int = PREC_FP64):
+        self._L = lib()
+        self.dim = dim
+        h = C.c_void_p()
+        self._check(self._L.mclccd_create(dim, C.byref(h)), None)
+        self._h = h
+        self.options = Options()
+        self.append_pair = None
+        self.append_discrete = None
+        self.filter_pair = None
+        self.narrow_phase = None
+        self._keep = []
+        self._last = None
+        if precision != PREC_FP64:
+            self.set_precision(precision)
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc, h):
+        if rc != OK:
+            L = self._L
+            msg = (L.mclccd_last_error(h) if h is not None else b"") or L.mclccd_status_string(rc)
+            raise CCDError(rc, msg.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.mclccd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _push_options(self):
+        o = self.options
+        self._check(self._L.mclccd_set_options(self._h, o.box_eta, o.vf_ccd_eta, o.ee_ccd_eta, o.flags()), self._h)
+
+    def _pull_options(self):
+        b, v, e, f = C.c_double(), C.c_double(), C.c_double(), C.c_uint()
+        self._L.mclccd_get_options(self._h, C.byref(b), C.byref(v), C.byref(e), C.byref(f))
+        self.options.box_eta, self.options.vf_ccd_eta, self.options.ee_ccd_eta = b.value, v.value, e.value
+
+    def set_precision(self, precision: int):
+        self._check(self._L.mclccd_set_precision(self._h, precision), self._h)
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self._L.mclccd_set_stream(self._h, C.c_void_p(stream_handle or 0)), self._h)
+
+    # -- the reference API --------------------------------------------------
+    def update(self, V0, V1, P, active=None):
+        """BVHTree::update (BVHTree.cpp:27-126)."""
+        pv0, k0, a0, nv = _arg(V0, np.float64, self.dim)
+        pv1, k1, a1, nv1 = _arg(V1, np.float64, self.dim)
+        pp, kp, ap, npr = _arg(P, np.int32)
+        pa, ka, aa, _ = _arg(active, np.int32)
+        if nv != nv1:   # BVHTree.hpp:160: silently ignored by the reference
+            raise ValueError("V0 and V1 must have the same number of rows")
+        kinds = {k for k in (k0, k1, kp, ka) if k is not None}
+        if len(kinds) > 1:
+            raise ValueError("V0, V1, P and active must all be host arrays or all CUDA tensors")
+        pdim = ap.shape[1] if ap.ndim == 2 else self.dim
+        self._push_options()
+        rc = self._L.mclccd_update(self._h, pv0, pv1, nv, pp, npr, pdim, pa, kinds.pop() if kinds else MEM_HOST)
+        self._pull_options()
+        self._check(rc, self._h)
+        self._keep = [a0, a1, ap, aa]
+
+    def traverse(self, V0=None, V1=None, P=None):
+        """BVHTree::traverse (BVHTree.cpp:129-159), then the hooks."""
+        pv0, k0, a0, nv = _arg(V0, np.float64, self.dim)
+        pv1, k1, a1, _ = _arg(V1, np.float64, self.dim)
+        pp, kp, ap, _ = _arg(P, np.int32)
+        kind = k0 if k0 is not None else MEM_HOST
+        self._push_options()
+        self._check(self._L.mclccd_traverse(self._h, pv0, pv1, nv, pp, kind), self._h)
+        self._dispatch(V0, V1)
+
+    def _dispatch(self, V0, V1):
+        if self.filter_pair is not None or self.narrow_phase is not None:
+            sten, is_vf = self.candidates()
+            keep = np.ones(len(sten), bool)
+            if self.filter_pair is not None:
+                for i in range(len(sten)):
+                    if self.filter_pair(sten[i], bool(is_vf[i])):
+                        keep[i] = False
+            sten, is_vf = sten[keep], is_vf[keep]
+            if self.narrow_phase is not None:
+                toi = np.array([self.narrow_phase(sten[i], bool(is_vf[i])) for i in range(len(sten))], np.float64)
+            else:
+                v0 = V0 if V0 is not None else self._keep[0]
+                v1 = V1 if V1 is not None else self._keep[1]
+                if _is_torch_cuda(v0):
+                    v0, v1 = v0.cpu().numpy(), v1.cpu().numpy()
+                toi, _ = narrow_phase_bulk(v0, v1, sten, is_vf, self.options.vf_ccd_eta, self.options.ee_ccd_eta)
+            m = toi >= 0
+            self._last = (sten[m], is_vf[m], toi[m])
+            if self.append_pair is not None:
+                for s, v, t in zip(*self._last):
+                    self.append_pair(s, bool(v), float(t))
+        elif self.append_pair is not None:
+            for s, v, t in zip(*self.hits()):
+                self.append_pair(s, bool(v), float(t))
+        if self.append_discrete is not None and self.options.discrete:
+            for a, b in self.discrete():
+                if self.append_discrete(int(a), int(b)):
+                    break
+
+    # -- array access -----------------------------------------------------
+    def counts(self) -> dict:
+        v = [C.c_longlong() for _ in range(5)]
+        self._check(self._L.mclccd_counts(self._h, *[C.byref(x) for x in v]), self._h)
+        return dict(zip(("hits", "discrete", "vf", "ee", "leaf_pairs"), (x.value for x in v)))
+
+    def hits(self):
+        """(sten int32[n,4], is_vf uint8[n], toi float64[n]) of the last traverse."""
+        if self._last is not None and (self.filter_pair is not None or self.narrow_phase is not None):
+            return self._last
+        n = self.counts()["hits"]
+        s = np.empty((n, 4), np.int32); v = np.empty(n, np.uint8); t = np.empty(n, np.float64)
+        self._check(self._L.mclccd_get_hits(self._h, MEM_HOST, n, s.ctypes.data, v.ctypes.data, t.ctypes.data), self._h)
+        return s, v, t
+
+    def discrete(self):
+        n = self.counts()["discrete"]
+        d = np.empty((n, 2), np.int32)
+        self._check(self._L.mclccd_get_discrete(self._h, MEM_HOST, n, d.ctypes.data), self._h)
+        return d
+
+    def candidates(self):
+        c = self.counts()
+        n = c["vf"] + c["ee"]
+        s = np.empty((n, 4), np.int32); v = np.empty(n, np.uint8)
+        self._check(self._L.mclccd_get_candidates(self._h, MEM_HOST, n, s.ctypes.data, v.ctypes.data), self._h)
+        return s, v
+
+    def leaves(self, np_: int):
+        b = np.empty((np_, 6, self.dim), np.float64); f = np.empty(np_, np.uint8)
+        self._check(self._L.mclccd_get_leaves(self._h, b.ctypes.data, f.ctypes.data), self._h)
+        return b, f
+
+    def stage_ms(self):
+        a = (C.c_float * 7)()
+        self._L.mclccd_stage_ms(self._h, a, 7)
+        return dict(zip(("update", "build", "refit", "traverse", "walk", "expand", "narrow"), list(a)))
+
+    def kernel_launches(self) -> int:
+        n = C.c_longlong()
+        self._L.mclccd_kernel_launches(self._h, C.byref(n))
+        return n.value
+
+
+def narrow_phase_bulk(V0, V1, sten, is_vf, vf_eta, ee_eta=None, stream: int | None = None):
+    """NarrowPhaseACCD::query_ccd_vf/ee over a stencil array on the GPU.
+    Returns (toi, hit); toi is -1 where hit == 0."""
+    L = lib()
+    ee_eta = vf_eta if ee_eta is None else ee_eta
+    if _is_torch_cuda(V0):
+        import torch
+        n = sten.shape[0]
+        dim = V0.shape[1]
+        toi = torch.empty(n, dtype=torch.float64, device=V0.device)
+        hit = torch.empty(n, dtype=torch.int32, device=V0.device)
+        rc = L.mclccd_narrow_phase_bulk(dim, V0.data_ptr(), V1.data_ptr(), V0.shape[0], sten.contiguous().data_ptr(),
+                                        is_vf.contiguous().data_ptr(), n, vf_eta, ee_eta, toi.data_ptr(),
+                                        hit.data_ptr(), MEM_DEVICE, C.c_void_p(stream or 0))
+    else:
+        V0 = np.ascontiguousarray(V0, np.float64); V1 = np.ascontiguousarray(V1, np.float64)
+        s = np.ascontiguousarray(sten, np.int32).reshape(-1, 4)
+        v = np.ascontiguousarray(is_vf, np.uint8).reshape(-1)
+        n = len(s)
+        toi = np.empty(n, np.float64); hit = np.empty(n, np.int32)
+        rc = L.mclccd_narrow_phase_bulk(V0.shape[1], V0.ctypes.data, V1.ctypes.data, V0.shape[0], s.ctypes.data,
+                                        v.ctypes.data, n, vf_eta, ee_eta, toi.ctypes.data, hit.ctypes.data,
+                                        MEM_HOST, C.c_void_p(stream or 0))
+    if rc != OK:
+        raise CCDError(rc, L.mclccd_status_string(rc).decode())
+    return toi, hit

@@ -1,0 +1,664 @@
+// C ABI of the B200 CCD path: handle state, device buffers and the
+// update / traverse orchestration (see include/mclccd_b200.h).
+#include "../../include/mclccd_b200.h"
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace mclccd;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+constexpr int kExpandGrid = 148 * 8;
+constexpr int kAccdGrid = 148 * 16;
+constexpr int kMaxAttempts = 3;
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+        else prev = -1;
+    }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+} // namespace
+
+struct mclccd_tree {
+    int dim = 3;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    double box_eta = 1e-6, vf_eta = 1e-6, ee_eta = 1e-6;
+    unsigned flags = MCLCCD_OPT_DEFAULT;
+    int precision = MCLCCD_PREC_FP64;
+    std::string err;
+
+    bool built = false, traversed = false;
+    int np = 0, pdim = 0, nv = 0, flags_np = 0;
+    const double *upd_V0 = nullptr, *upd_V1 = nullptr;
+    long long launches = 0;
+    float stage[7] = {0, 0, 0, 0, 0, 0, 0};
+    unsigned long long n_pairs = 0, n_vf = 0, n_ee = 0, n_hits = 0, n_disc = 0;
+    unsigned long long cap_pairs = 0, cap_vf = 0, cap_ee = 0, cap_hits = 0, cap_disc = 0;
+
+    DevBuf V0d, V1d, Pd, Pstage, actd, pflags, pflags_tmp, vowner, ekeys, eowner;
+    DevBuf cent, bounds, keys, vals, keys_alt, vals_alt, sort_scratch;
+    DevBuf nodes, leaf_parent, visits, leaf_box, leaf_active;
+    DevBuf pairs, vf, ee, hit_sten, hit_toi, hit_isvf, disc, counters, diff;
+    std::vector<DevBuf *> all()
+    {
+        return {&V0d, &V1d, &Pd, &Pstage, &actd, &pflags, &pflags_tmp, &vowner, &ekeys, &eowner, &cent, &bounds,
+                &keys, &vals, &keys_alt, &vals_alt, &sort_scratch, &nodes, &leaf_parent, &visits, &leaf_box,
+                &leaf_active, &pairs, &vf, &ee, &hit_sten, &hit_toi, &hit_isvf, &disc, &counters, &diff};
+    }
+    Counters *h_cnt = nullptr;   // pinned mirror of the device counters
+    int *h_diff = nullptr;
+    cudaEvent_t ev[8] = {};
+};
+
+namespace {
+
+int fail(mclccd_tree *t, int code, const std::string &msg)
+{
+    if (t) t->err = msg;
+    return code;
+}
+
+int cuda_fail(mclccd_tree *t, cudaError_t e, const char *what)
+{
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(t, e == cudaErrorMemoryAllocation ? MCLCCD_ERR_NOMEM : MCLCCD_ERR_CUDA, m);
+}
+
+#define MC_CUDA(t, x)                                        \
+    do {                                                     \
+        cudaError_t e_ = (x);                                \
+        if (e_ != cudaSuccess) return cuda_fail(t, e_, #x); \
+    } while (0)
+
+// Grow-only device buffer (contents are not preserved).
+cudaError_t ensure(DevBuf &b, size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    if (bytes <= b.cap) return cudaSuccess;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t want = bytes + bytes / 8;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) { cudaGetLastError(); return e; }
+    b.cap = want;
+    return cudaSuccess;
+}
+
+template <typename T> T *as(DevBuf &b) { return reinterpret_cast<T *>(b.p); }
+
+cudaMemcpyKind h2d_or_d2d(int mem_kind) { return mem_kind == MCLCCD_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice; }
+
+int check_launch(mclccd_tree *t, const char *what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(t, e, what);
+    return MCLCCD_OK;
+}
+
+int device_errors(mclccd_tree *t, unsigned err)
+{
+    if (err & kErrBadIndex) return fail(t, MCLCCD_ERR_INVALID, "a primitive or stencil references a vertex outside [0, nv)");
+    if (err & kErrHashFull) return fail(t, MCLCCD_ERR_DEVICE, "edge table probe limit reached");
+    if (err & kErrSortWait) return fail(t, MCLCCD_ERR_DEVICE, "radix sort look-back wait gave up");
+    if (err & kErrStack) return fail(t, MCLCCD_ERR_DEVICE, "traversal stack overflow");
+    return MCLCCD_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *mclccd_status_string(int s)
+{
+    switch (s) {
+    case MCLCCD_OK: return "ok";
+    case MCLCCD_ERR_INVALID: return "invalid argument";
+    case MCLCCD_ERR_CUDA: return "CUDA error";
+    case MCLCCD_ERR_NOMEM: return "out of device memory";
+    case MCLCCD_ERR_OVERFLOW: return "output capacity too small";
+    case MCLCCD_ERR_STATE: return "call out of order";
+    case MCLCCD_ERR_DEVICE: return "device-side failure (bounded wait or stack)";
+    case MCLCCD_ERR_UNSUPPORTED: return "unsupported option";
+    }
+    return "unknown status";
+}
+
+const char *mclccd_last_error(const mclccd_tree *t) { return t ? t->err.c_str() : "null handle"; }
+
+int mclccd_create(int dim, mclccd_tree **out)
+{
+    if (!out || (dim != 2 && dim != 3)) return MCLCCD_ERR_INVALID;
+    *out = nullptr;
+    mclccd_tree *t = new mclccd_tree();
+    t->dim = dim;
+    cudaError_t e = cudaGetDevice(&t->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&t->own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost(&t->h_cnt, sizeof(Counters));
+    if (e == cudaSuccess) e = cudaMallocHost(&t->h_diff, sizeof(int));
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&t->ev[i]);
+    if (e == cudaSuccess) e = ensure(t->counters, sizeof(Counters));
+    if (e == cudaSuccess) e = ensure(t->diff, sizeof(int));
+    if (e != cudaSuccess) {
+        mclccd_destroy(t);
+        return e == cudaErrorMemoryAllocation ? MCLCCD_ERR_NOMEM : MCLCCD_ERR_CUDA;
+    }
+    t->stream = t->own_stream;
+    *out = t;
+    return MCLCCD_OK;
+}
+
+int mclccd_destroy(mclccd_tree *t)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    DeviceGuard g(t->device);
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    for (DevBuf *b : t->all())
+        if (b->p) cudaFree(b->p);
+    for (int i = 0; i < 8; ++i)
+        if (t->ev[i]) cudaEventDestroy(t->ev[i]);
+    if (t->h_cnt) cudaFreeHost(t->h_cnt);
+    if (t->h_diff) cudaFreeHost(t->h_diff);
+    if (t->own_stream) cudaStreamDestroy(t->own_stream);
+    delete t;
+    return MCLCCD_OK;
+}
+
+int mclccd_set_options(mclccd_tree *t, double box_eta, double vf, double ee, unsigned flags)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!(box_eta >= 0) || !(vf >= 0) || !(ee >= 0)) return fail(t, MCLCCD_ERR_INVALID, "etas must be >= 0");
+    t->box_eta = box_eta;
+    t->vf_eta = vf;
+    t->ee_eta = ee;
+    t->flags = flags;
+    return MCLCCD_OK;
+}
+
+int mclccd_get_options(const mclccd_tree *t, double *box_eta, double *vf, double *ee, unsigned *flags)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (box_eta) *box_eta = t->box_eta;
+    if (vf) *vf = t->vf_eta;
+    if (ee) *ee = t->ee_eta;
+    if (flags) *flags = t->flags;
+    return MCLCCD_OK;
+}
+
+int mclccd_set_stream(mclccd_tree *t, void *stream)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    t->stream = stream ? static_cast<cudaStream_t>(stream) : t->own_stream;
+    return MCLCCD_OK;
+}
+
+int mclccd_set_precision(mclccd_tree *t, int precision)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (precision != MCLCCD_PREC_FP64 && precision != MCLCCD_PREC_FP32_CERTIFIED)
+        return fail(t, MCLCCD_ERR_INVALID, "unknown precision");
+    t->precision = precision;
+    return MCLCCD_OK;
+}
+
+int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, const int *P, int np, int pdim,
+                  const int *active, int mem_kind)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    t->err.clear();
+    if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
+    if (np < 0 || nv < 0) return fail(t, MCLCCD_ERR_INVALID, "negative size");
+    if (t->flags & MCLCCD_OPT_VF_ONE_SIDED)
+        return fail(t, MCLCCD_ERR_UNSUPPORTED, "vf_one_sided (CTCD narrow phase) is not provided");
+    if (!(t->box_eta >= 0) || !(t->vf_eta >= 0) || !(t->ee_eta >= 0)) return fail(t, MCLCCD_ERR_INVALID, "etas must be >= 0");
+    // BVHTree.cpp:39-40: the narrow-phase gaps never exceed the box padding.
+    t->vf_eta = std::min(t->vf_eta, t->box_eta);
+    t->ee_eta = std::min(t->ee_eta, t->box_eta);
+    t->traversed = false;
+    if (np == 0) {   // BVHTree.cpp:29-34: clear
+        t->built = true;
+        t->np = 0;
+        t->pdim = pdim;
+        t->nv = nv;
+        t->flags_np = 0;
+        return MCLCCD_OK;
+    }
+    if (!V0 || !V1 || !P || nv <= 0) return fail(t, MCLCCD_ERR_INVALID, "null array or nv == 0");
+    if (pdim < 1 || pdim > 4) return fail(t, MCLCCD_ERR_INVALID, "pdim must be in [1, 4]");
+    DeviceGuard g(t->device);
+    cudaStream_t st = t->stream;
+    const int dim = t->dim;
+    const bool prof = (t->flags & MCLCCD_OPT_PROFILE) != 0;
+    if (prof) cudaEventRecord(t->ev[0], st);
+
+    const double *dV0 = V0, *dV1 = V1;
+    const int *dact = active;
+    const size_t vbytes = sizeof(double) * (size_t)nv * dim;
+    if (mem_kind == MCLCCD_MEM_HOST) {
+        MC_CUDA(t, ensure(t->V0d, vbytes));
+        MC_CUDA(t, ensure(t->V1d, vbytes));
+        MC_CUDA(t, cudaMemcpyAsync(t->V0d.p, V0, vbytes, cudaMemcpyHostToDevice, st));
+        MC_CUDA(t, cudaMemcpyAsync(t->V1d.p, V1, vbytes, cudaMemcpyHostToDevice, st));
+        dV0 = as<double>(t->V0d);
+        dV1 = as<double>(t->V1d);
+        if (active) {
+            MC_CUDA(t, ensure(t->actd, sizeof(int) * (size_t)nv));
+            MC_CUDA(t, cudaMemcpyAsync(t->actd.p, active, sizeof(int) * (size_t)nv, cudaMemcpyHostToDevice, st));
+            dact = as<int>(t->actd);
+        }
+    }
+    const long long pcount = (long long)np * pdim;
+    MC_CUDA(t, ensure(t->Pstage, sizeof(int) * (size_t)pcount));
+    MC_CUDA(t, cudaMemcpyAsync(t->Pstage.p, P, sizeof(int) * (size_t)pcount, h2d_or_d2d(mem_kind), st));
+    MC_CUDA(t, cudaMemsetAsync(t->counters.p, 0, sizeof(Counters), st));
+
+    // Refit-only when the topology is byte-identical to the previous update.
+    bool same = t->built && t->np > 1 && !(t->flags & MCLCCD_OPT_ALWAYS_REBUILD) && np == t->np &&
+                pdim == t->pdim && nv == t->nv;
+    if (same) {
+        MC_CUDA(t, cudaMemsetAsync(t->diff.p, 0, sizeof(int), st));
+        launch_compare(as<int>(t->Pstage), as<int>(t->Pd), pcount, as<int>(t->diff), st);
+        ++t->launches;
+        MC_CUDA(t, cudaMemcpyAsync(t->h_diff, t->diff.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MC_CUDA(t, cudaStreamSynchronize(st));
+        same = *t->h_diff == 0;
+    }
+    std::swap(t->Pstage, t->Pd);
+    const int *dP = as<int>(t->Pd);
+    Counters *cnt = as<Counters>(t->counters);
+
+    // Representative flags: recomputed only when the primitive count changes
+    // (BVHTree.cpp:44-48); new leaves default to "all represented" and old
+    // leaves keep their flags when reptri is off (BVHLeaf.hpp:45-49).
+    if (np != t->flags_np) {
+        MC_CUDA(t, ensure(t->pflags_tmp, (size_t)np));
+        MC_CUDA(t, cudaMemsetAsync(t->pflags_tmp.p, (int)kFlagAllRep, (size_t)np, st));
+        if (t->flags_np > 0 && t->pflags.p)
+            MC_CUDA(t, cudaMemcpyAsync(t->pflags_tmp.p, t->pflags.p, (size_t)std::min(np, t->flags_np),
+                                       cudaMemcpyDeviceToDevice, st));
+        std::swap(t->pflags, t->pflags_tmp);
+        if ((t->flags & MCLCCD_OPT_REPTRI) && (pdim == 2 || pdim == 3)) {
+            unsigned long long ecap = 1024;
+            while (ecap < (unsigned long long)pcount * 2) ecap <<= 1;
+            MC_CUDA(t, ensure(t->vowner, sizeof(int) * (size_t)nv));
+            if (pdim == 3) {
+                MC_CUDA(t, ensure(t->ekeys, sizeof(unsigned long long) * ecap));
+                MC_CUDA(t, ensure(t->eowner, sizeof(int) * ecap));
+            }
+            launch_owner_flags(dP, np, pdim, nv, as<int>(t->vowner), as<unsigned long long>(t->ekeys),
+                               as<int>(t->eowner), ecap, as<unsigned char>(t->pflags), cnt, st);
+            t->launches += 2;
+        }
+        t->flags_np = np;
+    }
+
+    if (!same) {
+        MC_CUDA(t, ensure(t->cent, sizeof(float) * (size_t)np * dim));
+        MC_CUDA(t, ensure(t->bounds, sizeof(unsigned) * 8));
+        MC_CUDA(t, ensure(t->keys, sizeof(unsigned) * (size_t)np));
+        MC_CUDA(t, ensure(t->vals, sizeof(int) * (size_t)np));
+        MC_CUDA(t, ensure(t->keys_alt, sizeof(unsigned) * (size_t)np));
+        MC_CUDA(t, ensure(t->vals_alt, sizeof(int) * (size_t)np));
+        MC_CUDA(t, ensure(t->sort_scratch, sort_scratch_bytes(np, sort_num_passes(30))));
+        MC_CUDA(t, ensure(t->nodes, sizeof(Node) * (size_t)std::max(1, np - 1)));
+        MC_CUDA(t, ensure(t->leaf_parent, sizeof(int) * (size_t)np));
+        launch_centroids(dim, dV0, dV1, dP, np, pdim, nv, as<float>(t->cent), as<unsigned>(t->bounds), cnt, st);
+        launch_morton(dim, as<float>(t->cent), np, as<unsigned>(t->bounds), as<unsigned>(t->keys), as<int>(t->vals), st);
+        launch_sort_pairs(as<unsigned>(t->keys), as<int>(t->vals), as<unsigned>(t->keys_alt), as<int>(t->vals_alt), np,
+                          30, t->sort_scratch.p, cnt, st);
+        launch_karras(as<unsigned>(t->keys), np, as<Node>(t->nodes), as<int>(t->leaf_parent), st);
+        t->launches += 4 + 1 + sort_num_passes(30) + (np > 1 ? 1 : 0);
+        if (int rc = check_launch(t, "build kernels")) return rc;
+    }
+    if (prof) cudaEventRecord(t->ev[1], st);
+    MC_CUDA(t, ensure(t->leaf_box, sizeof(double) * 4 * dim * (size_t)np));
+    MC_CUDA(t, ensure(t->leaf_active, (size_t)np));
+    MC_CUDA(t, ensure(t->visits, sizeof(int) * (size_t)std::max(1, np - 1)));
+    launch_refit(dim, dV0, dV1, dP, np, pdim, nv, t->box_eta, dact, as<int>(t->vals), as<int>(t->leaf_parent),
+                 as<Node>(t->nodes), as<int>(t->visits), t->leaf_box.p, as<unsigned char>(t->leaf_active), cnt, st);
+    ++t->launches;
+    if (int rc = check_launch(t, "refit kernel")) return rc;
+    if (prof) cudaEventRecord(t->ev[2], st);
+    MC_CUDA(t, cudaMemcpyAsync(t->h_cnt, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    MC_CUDA(t, cudaStreamSynchronize(st));
+    if (prof) {
+        cudaEventElapsedTime(&t->stage[0], t->ev[0], t->ev[2]);
+        cudaEventElapsedTime(&t->stage[1], t->ev[0], t->ev[1]);
+        cudaEventElapsedTime(&t->stage[2], t->ev[1], t->ev[2]);
+    }
+    t->np = np;
+    t->pdim = pdim;
+    t->nv = nv;
+    t->upd_V0 = dV0;
+    t->upd_V1 = dV1;
+    const unsigned derr = t->h_cnt->err;
+    t->built = derr == 0;
+    if (derr) return device_errors(t, derr);
+    return MCLCCD_OK;
+}
+
+int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, const int *P, int mem_kind)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    t->err.clear();
+    if (!t->built) return fail(t, MCLCCD_ERR_STATE, "traverse before a successful update");
+    if (t->flags & MCLCCD_OPT_VF_ONE_SIDED)
+        return fail(t, MCLCCD_ERR_UNSUPPORTED, "vf_one_sided (CTCD narrow phase) is not provided");
+    if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
+    t->n_pairs = t->n_vf = t->n_ee = t->n_hits = t->n_disc = 0;
+    t->traversed = true;
+    if (t->np <= 1) return MCLCCD_OK;   // BVHTree.cpp:131-132
+    const int dim = t->dim;
+    if (t->pdim != dim)
+        return fail(t, MCLCCD_ERR_INVALID, "traverse needs P as triangles (3D) or edges (2D): pdim must equal dim");
+    DeviceGuard g(t->device);
+    cudaStream_t st = t->stream;
+    const bool prof = (t->flags & MCLCCD_OPT_PROFILE) != 0;
+    if (prof) cudaEventRecord(t->ev[3], st);
+
+    const double *dV0, *dV1;
+    const int *dP;
+    if (!V0 && !V1 && !P) {
+        dV0 = t->upd_V0;
+        dV1 = t->upd_V1;
+        dP = as<int>(t->Pd);
+        nv = t->nv;
+    } else {
+        if (!V0 || !V1 || !P) return fail(t, MCLCCD_ERR_INVALID, "V0, V1, P must all be given (or all NULL)");
+        if (nv <= 0) nv = t->nv;
+        dV0 = V0;
+        dV1 = V1;
+        dP = P;
+        if (mem_kind == MCLCCD_MEM_HOST) {
+            const size_t vbytes = sizeof(double) * (size_t)nv * dim;
+            const size_t pbytes = sizeof(int) * (size_t)t->np * dim;
+            MC_CUDA(t, ensure(t->V0d, vbytes));
+            MC_CUDA(t, ensure(t->V1d, vbytes));
+            MC_CUDA(t, ensure(t->Pstage, pbytes));
+            MC_CUDA(t, cudaMemcpyAsync(t->V0d.p, V0, vbytes, cudaMemcpyHostToDevice, st));
+            MC_CUDA(t, cudaMemcpyAsync(t->V1d.p, V1, vbytes, cudaMemcpyHostToDevice, st));
+            MC_CUDA(t, cudaMemcpyAsync(t->Pstage.p, P, pbytes, cudaMemcpyHostToDevice, st));
+            dV0 = as<double>(t->V0d);
+            dV1 = as<double>(t->V1d);
+            dP = as<int>(t->Pstage);
+            t->upd_V0 = dV0;   // the update's copies were overwritten
+            t->upd_V1 = dV1;
+        }
+    }
+    const int np = t->np;
+    const bool cont = (t->flags & MCLCCD_OPT_CONTINUOUS) != 0;
+    const bool discr = (t->flags & MCLCCD_OPT_DISCRETE) != 0;
+    if (t->cap_pairs == 0) {
+        t->cap_pairs = std::max<unsigned long long>(4096, 8ull * np);
+        t->cap_vf = std::max<unsigned long long>(4096, 8ull * np);
+        t->cap_ee = std::max<unsigned long long>(4096, dim == 3 ? 16ull * np : 16);
+        t->cap_hits = t->cap_vf + t->cap_ee;
+        t->cap_disc = std::max<unsigned long long>(1024, np / 4);
+    }
+    Counters *cnt = as<Counters>(t->counters);
+    for (int attempt = 0;; ++attempt) {
+        MC_CUDA(t, ensure(t->pairs, sizeof(int2) * t->cap_pairs));
+        MC_CUDA(t, ensure(t->vf, sizeof(int4) * t->cap_vf));
+        MC_CUDA(t, ensure(t->ee, sizeof(int4) * t->cap_ee));
+        MC_CUDA(t, ensure(t->hit_sten, sizeof(int4) * t->cap_hits));
+        MC_CUDA(t, ensure(t->hit_toi, sizeof(double) * t->cap_hits));
+        MC_CUDA(t, ensure(t->hit_isvf, t->cap_hits));
+        MC_CUDA(t, ensure(t->disc, sizeof(int2) * t->cap_disc));
+        MC_CUDA(t, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
+        launch_traverse(dim, as<Node>(t->nodes), t->leaf_box.p, as<unsigned char>(t->leaf_active), as<int>(t->vals), np,
+                        as<int2>(t->pairs), t->cap_pairs, cnt, st);
+        if (prof) cudaEventRecord(t->ev[4], st);
+        launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                            as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
+                            cont, discr, cnt, kExpandGrid, st);
+        if (prof) cudaEventRecord(t->ev[5], st);
+        t->launches += 2;
+        if (cont) {
+            launch_accd_pipeline(dim, true, as<int4>(t->vf), &cnt->n_vf, t->cap_vf, dV0, dV1, nv, t->vf_eta,
+                                 as<int4>(t->hit_sten), as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf),
+                                 t->cap_hits, cnt, kAccdGrid, st);
+            ++t->launches;
+            if (dim == 3) {
+                launch_accd_pipeline(dim, false, as<int4>(t->ee), &cnt->n_ee, t->cap_ee, dV0, dV1, nv, t->ee_eta,
+                                     as<int4>(t->hit_sten), as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf),
+                                     t->cap_hits, cnt, kAccdGrid, st);
+                ++t->launches;
+            }
+        }
+        if (prof) cudaEventRecord(t->ev[6], st);
+        if (int rc = check_launch(t, "traverse kernels")) return rc;
+        MC_CUDA(t, cudaMemcpyAsync(t->h_cnt, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        MC_CUDA(t, cudaStreamSynchronize(st));
+        const Counters &c = *t->h_cnt;
+        bool grow = false;
+        auto need = [&](unsigned long long count, unsigned long long &cap) {
+            if (count > cap) { cap = count + count / 4 + 1024; grow = true; }
+        };
+        need(c.n_pairs, t->cap_pairs);
+        need(c.n_vf, t->cap_vf);
+        need(c.n_ee, t->cap_ee);
+        need(c.n_hits, t->cap_hits);
+        need(c.n_discrete, t->cap_disc);
+        if (!grow) break;
+        if (attempt + 1 >= kMaxAttempts) return fail(t, MCLCCD_ERR_DEVICE, "result buffers kept overflowing");
+    }
+    const Counters &c = *t->h_cnt;
+    if (prof) {
+        cudaEventElapsedTime(&t->stage[3], t->ev[3], t->ev[6]);
+        cudaEventElapsedTime(&t->stage[4], t->ev[3], t->ev[4]);
+        cudaEventElapsedTime(&t->stage[5], t->ev[4], t->ev[5]);
+        cudaEventElapsedTime(&t->stage[6], t->ev[5], t->ev[6]);
+    }
+    t->n_pairs = c.n_pairs;
+    t->n_vf = c.n_vf;
+    t->n_ee = c.n_ee;
+    t->n_hits = c.n_hits;
+    t->n_disc = c.n_discrete;
+    if (c.err) {
+        t->traversed = false;
+        return device_errors(t, c.err);
+    }
+    return MCLCCD_OK;
+}
+
+int mclccd_counts(const mclccd_tree *t, long long *n_hits, long long *n_discrete, long long *n_vf, long long *n_ee,
+                  long long *n_leaf_pairs)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!t->traversed) return MCLCCD_ERR_STATE;
+    if (n_hits) *n_hits = (long long)t->n_hits;
+    if (n_discrete) *n_discrete = (long long)t->n_disc;
+    if (n_vf) *n_vf = (long long)t->n_vf;
+    if (n_ee) *n_ee = (long long)t->n_ee;
+    if (n_leaf_pairs) *n_leaf_pairs = (long long)t->n_pairs;
+    return MCLCCD_OK;
+}
+
+static int copy_out(mclccd_tree *t, void *dst, const void *src, size_t bytes, int mem_kind)
+{
+    if (!dst || bytes == 0) return MCLCCD_OK;
+    cudaMemcpyKind k = mem_kind == MCLCCD_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    MC_CUDA(t, cudaMemcpyAsync(dst, src, bytes, k, t->stream));
+    return MCLCCD_OK;
+}
+
+int mclccd_get_hits(mclccd_tree *t, int mem_kind, long long capacity, int *sten, unsigned char *is_vf, double *toi)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!t->traversed) return fail(t, MCLCCD_ERR_STATE, "no traverse results");
+    if (capacity < 0 || (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE)) return MCLCCD_ERR_INVALID;
+    DeviceGuard g(t->device);
+    const size_t n = (size_t)std::min<unsigned long long>(t->n_hits, (unsigned long long)capacity);
+    if (int rc = copy_out(t, sten, t->hit_sten.p, sizeof(int4) * n, mem_kind)) return rc;
+    if (int rc = copy_out(t, is_vf, t->hit_isvf.p, n, mem_kind)) return rc;
+    if (int rc = copy_out(t, toi, t->hit_toi.p, sizeof(double) * n, mem_kind)) return rc;
+    MC_CUDA(t, cudaStreamSynchronize(t->stream));
+    return n < t->n_hits ? MCLCCD_ERR_OVERFLOW : MCLCCD_OK;
+}
+
+int mclccd_get_discrete(mclccd_tree *t, int mem_kind, long long capacity, int *pairs)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!t->traversed) return fail(t, MCLCCD_ERR_STATE, "no traverse results");
+    if (capacity < 0 || (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE)) return MCLCCD_ERR_INVALID;
+    DeviceGuard g(t->device);
+    const size_t n = (size_t)std::min<unsigned long long>(t->n_disc, (unsigned long long)capacity);
+    if (int rc = copy_out(t, pairs, t->disc.p, sizeof(int2) * n, mem_kind)) return rc;
+    MC_CUDA(t, cudaStreamSynchronize(t->stream));
+    return n < t->n_disc ? MCLCCD_ERR_OVERFLOW : MCLCCD_OK;
+}
+
+int mclccd_get_candidates(mclccd_tree *t, int mem_kind, long long capacity, int *sten, unsigned char *is_vf)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!t->traversed) return fail(t, MCLCCD_ERR_STATE, "no traverse results");
+    if (capacity < 0 || (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE)) return MCLCCD_ERR_INVALID;
+    DeviceGuard g(t->device);
+    const unsigned long long total = t->n_vf + t->n_ee;
+    const size_t nvf = (size_t)std::min<unsigned long long>(t->n_vf, (unsigned long long)capacity);
+    const size_t nee = (size_t)std::min<unsigned long long>(t->n_ee, (unsigned long long)capacity - nvf);
+    if (int rc = copy_out(t, sten, t->vf.p, sizeof(int4) * nvf, mem_kind)) return rc;
+    if (sten) if (int rc = copy_out(t, sten + 4 * nvf, t->ee.p, sizeof(int4) * nee, mem_kind)) return rc;
+    if (is_vf) {
+        if (mem_kind == MCLCCD_MEM_HOST) {
+            std::memset(is_vf, 1, nvf);
+            std::memset(is_vf + nvf, 0, nee);
+        } else {
+            MC_CUDA(t, cudaMemsetAsync(is_vf, 1, nvf, t->stream));
+            MC_CUDA(t, cudaMemsetAsync(is_vf + nvf, 0, nee, t->stream));
+        }
+    }
+    MC_CUDA(t, cudaStreamSynchronize(t->stream));
+    return nvf + nee < total ? MCLCCD_ERR_OVERFLOW : MCLCCD_OK;
+}
+
+int mclccd_get_leaves(mclccd_tree *t, double *boxes, unsigned char *flags)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!t->built) return fail(t, MCLCCD_ERR_STATE, "no update");
+    DeviceGuard g(t->device);
+    const int np = t->np, dim = t->dim;
+    if (np == 0) return MCLCCD_OK;
+    std::vector<double> lb((size_t)np * 4 * dim);
+    std::vector<int> sorted(np);
+    std::vector<unsigned char> act(np), fl(np);
+    MC_CUDA(t, cudaMemcpyAsync(lb.data(), t->leaf_box.p, lb.size() * sizeof(double), cudaMemcpyDeviceToHost, t->stream));
+    MC_CUDA(t, cudaMemcpyAsync(sorted.data(), t->vals.p, sizeof(int) * np, cudaMemcpyDeviceToHost, t->stream));
+    MC_CUDA(t, cudaMemcpyAsync(act.data(), t->leaf_active.p, np, cudaMemcpyDeviceToHost, t->stream));
+    MC_CUDA(t, cudaMemcpyAsync(fl.data(), t->pflags.p, np, cudaMemcpyDeviceToHost, t->stream));
+    MC_CUDA(t, cudaStreamSynchronize(t->stream));
+    for (int k = 0; k < np; ++k) {
+        const int prim = sorted[k];
+        const double *s = &lb[(size_t)k * 4 * dim];   // lo0, hi0, lo1, hi1
+        if (boxes) {
+            double *b = boxes + (size_t)prim * 6 * dim;
+            for (int c = 0; c < dim; ++c) {
+                const double lo0 = s[c], hi0 = s[dim + c], lo1 = s[2 * dim + c], hi1 = s[3 * dim + c];
+                b[c] = lo0 < lo1 ? lo0 : lo1;
+                b[dim + c] = hi0 < hi1 ? hi1 : hi0;
+                b[2 * dim + c] = lo0;
+                b[3 * dim + c] = hi0;
+                b[4 * dim + c] = lo1;
+                b[5 * dim + c] = hi1;
+            }
+        }
+        if (flags) flags[prim] = (unsigned char)((fl[prim] & kFlagAllRep) | (act[k] ? kFlagActive : 0));
+    }
+    return MCLCCD_OK;
+}
+
+int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv, const int *sten,
+                             const unsigned char *is_vf, long long n, double vf_eta, double ee_eta, double *out_toi,
+                             int *out_hit, int mem_kind, void *stream)
+{
+    if ((dim != 2 && dim != 3) || n < 0 || nv < 0) return MCLCCD_ERR_INVALID;
+    if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return MCLCCD_ERR_INVALID;
+    if (!(vf_eta >= 0) || !(ee_eta >= 0)) return MCLCCD_ERR_INVALID;
+    if (n == 0) return MCLCCD_OK;
+    if (!V0 || !V1 || !sten || !is_vf || !out_toi || !out_hit || nv == 0) return MCLCCD_ERR_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t vbytes = sizeof(double) * (size_t)nv * dim;
+    // Scratch: the device error word, plus device copies of host arrays.
+    char *scratch = nullptr;
+    size_t off_cnt = 0, off_v0 = 256, off_v1 = 0, off_s = 0, off_f = 0, off_t = 0, off_h = 0, total = 256;
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    if (mem_kind == MCLCCD_MEM_HOST) {
+        off_v1 = off_v0 + align(vbytes);
+        off_s = off_v1 + align(vbytes);
+        off_f = off_s + align(sizeof(int) * 4 * (size_t)n);
+        off_t = off_f + align((size_t)n);
+        off_h = off_t + align(sizeof(double) * (size_t)n);
+        total = off_h + align(sizeof(int) * (size_t)n);
+    }
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&scratch), total, st);
+    if (e != cudaSuccess) { cudaGetLastError(); return e == cudaErrorMemoryAllocation ? MCLCCD_ERR_NOMEM : MCLCCD_ERR_CUDA; }
+    Counters *cnt = reinterpret_cast<Counters *>(scratch + off_cnt);
+    const double *dV0 = V0, *dV1 = V1;
+    const int *ds = sten;
+    const unsigned char *df = is_vf;
+    double *dt = out_toi;
+    int *dh = out_hit;
+    int rc = MCLCCD_OK;
+    e = cudaMemsetAsync(cnt, 0, sizeof(Counters), st);
+    if (e == cudaSuccess && mem_kind == MCLCCD_MEM_HOST) {
+        dV0 = reinterpret_cast<const double *>(scratch + off_v0);
+        dV1 = reinterpret_cast<const double *>(scratch + off_v1);
+        ds = reinterpret_cast<const int *>(scratch + off_s);
+        df = reinterpret_cast<const unsigned char *>(scratch + off_f);
+        dt = reinterpret_cast<double *>(scratch + off_t);
+        dh = reinterpret_cast<int *>(scratch + off_h);
+        e = cudaMemcpyAsync((void *)dV0, V0, vbytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync((void *)dV1, V1, vbytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync((void *)ds, sten, sizeof(int) * 4 * (size_t)n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync((void *)df, is_vf, (size_t)n, cudaMemcpyHostToDevice, st);
+    }
+    if (e == cudaSuccess) {
+        launch_accd_bulk(dim, ds, df, n, dV0, dV1, nv, vf_eta, ee_eta, dt, dh, cnt, st);
+        e = cudaGetLastError();
+    }
+    Counters h{};
+    if (e == cudaSuccess && mem_kind == MCLCCD_MEM_HOST) {
+        e = cudaMemcpyAsync(out_toi, dt, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out_hit, dh, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFreeAsync(scratch, st);
+    if (e != cudaSuccess) rc = MCLCCD_ERR_CUDA;
+    else if (h.err & kErrBadIndex) rc = MCLCCD_ERR_INVALID;
+    return rc;
+}
+
+int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)
+{
+    if (!t || !ms || n < 0) return -1;
+    int k = std::min(n, 7);
+    for (int i = 0; i < k; ++i) ms[i] = t->stage[i];
+    return k;
+}
+
+int mclccd_kernel_launches(const mclccd_tree *t, long long *n)
+{
+    if (!t || !n) return MCLCCD_ERR_INVALID;
+    *n = t->launches;
+    return MCLCCD_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,116 @@
+// Shared device-side definitions for the B200 CCD path.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mclccd {
+
+// ---------------------------------------------------------------------------
+// Per-primitive flags (uint8).  Bits 0-2: vertex slot j is the representative
+// occurrence of its vertex; bits 3-5: edge slot j is the representative
+// occurrence of its edge (mclccd BVHTree.cpp:50-80); bit 6: primitive active.
+// ---------------------------------------------------------------------------
+constexpr unsigned kFlagV0 = 1u;
+constexpr unsigned kFlagE0 = 1u << 3;
+constexpr unsigned kFlagActive = 1u << 6;
+constexpr unsigned kFlagAllRep = 0x3Fu;
+
+// Error bits accumulated on the device (Counters::err).  None of them traps:
+// the kernel records the bit and skips the offending access.
+constexpr unsigned kErrBadIndex = 1u << 0;    // a P entry outside [0, nv)
+constexpr unsigned kErrStack = 1u << 1;       // traversal stack overflow
+constexpr unsigned kErrSortWait = 1u << 2;    // radix-sort look-back gave up
+constexpr unsigned kErrHashFull = 1u << 3;    // edge hash table probe limit
+constexpr unsigned kErrAccdIters = 1u << 4;   // ACCD loop hit its 1000 cap (reported, result kept)
+
+// Device counters of one traverse: counts are exact even when a buffer is
+// too small (writes past capacity are skipped, the count keeps going).
+struct Counters {
+    unsigned long long n_pairs;
+    unsigned long long n_vf;
+    unsigned long long n_ee;
+    unsigned long long n_hits;
+    unsigned long long n_discrete;
+    unsigned long long n_certified;   // FP32 form: stencils decided in FP64
+    unsigned int err;
+    unsigned int pad;
+};
+
+// ---------------------------------------------------------------------------
+// Hierarchy layout (LBVH, Karras 2012).  Internal node i has children
+// split and split+1; each child is a leaf (sorted position) or an internal
+// node.  The children's FP32 swept boxes live in the parent, so one 64-byte
+// node read tests both children.
+//   3D: a = (lo_l.x, lo_l.y, lo_l.z, hi_l.x)  b = (hi_l.y, hi_l.z, lo_r.x, lo_r.y)
+//       c = (lo_r.z, hi_r.x, hi_r.y, hi_r.z)
+//   2D: a = (lo_l.x, lo_l.y, hi_l.x, hi_l.y)  b = (lo_r.x, lo_r.y, hi_r.x, hi_r.y)
+//   d = (split, meta, last, parent)
+// meta byte 0: bit0 left child is a leaf, bit1 right child is a leaf;
+// byte 1: left child active; byte 2: right child active.
+// ---------------------------------------------------------------------------
+struct __align__(16) Node {
+    float4 a, b, c;
+    int4 d;
+};
+constexpr int kMetaLeftLeaf = 1;
+constexpr int kMetaRightLeaf = 2;
+
+// FP64 leaf record in sorted order: t0 box then t1 box, each (min, max).
+// 3D: 12 doubles; 2D: 8 doubles.  The swept box is min/max of the two: the
+// reference pads the swept box, t0 and t1 boxes by the same eta, and
+// fl(min(a,b) - eta) == min(fl(a - eta), fl(b - eta)) for round-to-nearest.
+template <int DIM>
+struct LeafBox {
+    double lo0[DIM], hi0[DIM], lo1[DIM], hi1[DIM];
+};
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// Warp-aggregated append: every lane that calls this together (the active
+// lanes at this point) gets a distinct slot; one atomic per warp.
+__device__ __forceinline__ unsigned long long warp_append(unsigned long long *counter)
+{
+    unsigned mask = __activemask();
+    int leader = __ffs(mask) - 1;
+    unsigned rank = __popc(mask & lanemask_lt());
+    unsigned long long base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(counter, (unsigned long long)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + rank;
+}
+
+// Warp-wide (all 32 lanes must call) reservation of k slots per lane.
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *counter, unsigned k)
+{
+    unsigned incl = k;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)lane_id() >= o) incl += v;
+    }
+    unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long base = 0;
+    if (lane_id() == 31 && total) base = atomicAdd(counter, (unsigned long long)total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    return base + (incl - k);
+}
+
+// Monotone float <-> uint mapping for atomic min/max of floats.
+__device__ __forceinline__ unsigned float_to_ordered(float f)
+{
+    unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float ordered_to_float(unsigned u)
+{
+    unsigned v = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(v);
+#else
+    float f; __builtin_memcpy(&f, &v, 4); return f;
+#endif
+}
+
+} // namespace mclccd

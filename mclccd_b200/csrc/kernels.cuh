@@ -1,0 +1,43 @@
+// Host-callable kernel launchers (internal to libmclccd_b200.so).
+#pragma once
+
+#include "common.cuh"
+#include <cstddef>
+
+namespace mclccd {
+
+// build.cu
+void launch_centroids(int dim, const double *V0, const double *V1, const int *P, int np, int pdim, int nv,
+                      float *cent, unsigned *bounds, Counters *cnt, cudaStream_t st);
+void launch_morton(int dim, const float *cent, int np, const unsigned *bounds, unsigned *keys, int *vals, cudaStream_t st);
+void launch_karras(const unsigned *keys, int n, Node *nodes, int *leaf_parent, cudaStream_t st);
+void launch_refit(int dim, const double *V0, const double *V1, const int *P, int np, int pdim, int nv, double eta,
+                  const int *active, const int *sorted, const int *leaf_parent, Node *nodes, int *visits,
+                  void *leaf_box, unsigned char *leaf_active, Counters *cnt, cudaStream_t st);
+void launch_owner_flags(const int *P, int np, int pdim, int nv, int *vowner, unsigned long long *ekeys, int *eowner,
+                        unsigned long long ecap, unsigned char *flags, Counters *cnt, cudaStream_t st);
+void launch_compare(const int *a, const int *b, long long n, int *diff, cudaStream_t st);
+
+// sort.cu
+int sort_num_passes(unsigned key_bits);
+size_t sort_scratch_bytes(int n, int passes);
+void launch_sort_pairs(unsigned *keys, int *vals, unsigned *keys_alt, int *vals_alt, int n, unsigned key_bits,
+                       void *scratch, Counters *cnt, cudaStream_t st);
+
+// traverse.cu
+void launch_traverse(int dim, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
+                     const int *sorted, int n, int2 *pairs, unsigned long long cap, Counters *cnt, cudaStream_t st);
+void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,
+                         const unsigned char *flags, const double *V1, int nv, int4 *vf, unsigned long long vf_cap,
+                         int4 *ee, unsigned long long ee_cap, int2 *disc, unsigned long long disc_cap, int continuous,
+                         int discrete, Counters *cnt, int grid, cudaStream_t st);
+
+// narrow.cu
+void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
+                          const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
+                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st);
+void launch_accd_bulk(int dim, const int *sten, const unsigned char *is_vf, long long n, const double *V0,
+                      const double *V1, int nv, double vf_eta, double ee_eta, double *out_toi, int *out_hit,
+                      Counters *cnt, cudaStream_t st);
+
+} // namespace mclccd

@@ -1,0 +1,113 @@
+// FP64 ACCD narrow phase over stencil buffers.
+//
+// Replaces BVHTree::default_narrow_phase (BVHTree.cpp:429-461) ->
+// NarrowPhaseACCD::query_ccd_vf/ee -> additive_ccd (NarrowPhase.cpp:609-711).
+// One thread per stencil: gather 2 x (DIM+1) vertices, run ACCD, and either
+// append hits to the compacted contact buffer (warp-aggregated) or write the
+// per-stencil (toi, hit) of the bulk call.  Compiled with -fmad=false.
+#include "common.cuh"
+#include "geom.cuh"
+#include "kernels.cuh"
+
+namespace mclccd {
+
+template <int DIM>
+__device__ __forceinline__ bool gather_stencil(const int *s, const double *__restrict__ V0, const double *__restrict__ V1,
+                                               int nv, double (&x0)[DIM + 1][DIM], double (&x1)[DIM + 1][DIM])
+{
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < DIM + 1; ++i) {
+        int v = s[i];
+        if (v < 0 || v >= nv) { ok = false; v = 0; }
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            x0[i][k] = __ldg(V0 + (size_t)v * DIM + k);
+            x1[i][k] = __ldg(V1 + (size_t)v * DIM + k);
+        }
+    }
+    return ok;
+}
+
+// Pipeline form: stencils from the expansion kernel, count read on device.
+template <int DIM, bool VF>
+__global__ void __launch_bounds__(128)
+k_accd_pipeline(const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
+                const double *__restrict__ V0, const double *__restrict__ V1, int nv, double eta,
+                int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,
+                unsigned long long hit_cap, Counters *cnt)
+{
+    unsigned long long n = *(volatile const unsigned long long *)n_ptr;
+    if (n > cap) n = cap;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int4 s4 = sten[i];
+        const int s[4] = {s4.x, s4.y, s4.z, s4.w};
+        double x0[DIM + 1][DIM], x1[DIM + 1][DIM];
+        if (!gather_stencil<DIM>(s, V0, V1, nv, x0, x1)) { atomicOr(&cnt->err, kErrBadIndex); continue; }
+        double toi = -1.0;
+        int iters;
+        const int hit = accd<DIM, VF>(x0, x1, eta, toi, iters);
+        if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
+        if (hit) {
+            const unsigned long long slot = warp_append(&cnt->n_hits);
+            if (slot < hit_cap) {
+                hit_sten[slot] = s4;
+                hit_toi[slot] = toi;
+                hit_isvf[slot] = VF ? 1 : 0;
+            }
+        }
+    }
+}
+
+// Bulk form: caller-given stencils (int32 x 4 each, any alignment), per-stencil
+// outputs in input order.  toi = -1 on a miss, as default_narrow_phase returns.
+template <int DIM>
+__global__ void __launch_bounds__(128)
+k_accd_bulk(const int *__restrict__ sten, const unsigned char *__restrict__ is_vf, long long n,
+            const double *__restrict__ V0, const double *__restrict__ V1, int nv, double vf_eta, double ee_eta,
+            double *__restrict__ out_toi, int *__restrict__ out_hit, Counters *cnt)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int s[4] = {sten[4 * i], sten[4 * i + 1], sten[4 * i + 2], sten[4 * i + 3]};
+        double x0[DIM + 1][DIM], x1[DIM + 1][DIM];
+        double toi = -1.0;
+        int hit = 0, iters = 0;
+        if (!gather_stencil<DIM>(s, V0, V1, nv, x0, x1)) {
+            atomicOr(&cnt->err, kErrBadIndex);
+        } else if (DIM == 3 && !is_vf[i]) {
+            hit = accd<DIM, false>(x0, x1, ee_eta, toi, iters);
+        } else {
+            hit = accd<DIM, true>(x0, x1, vf_eta, toi, iters);
+        }
+        if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
+        out_toi[i] = hit ? toi : -1.0;
+        out_hit[i] = hit;
+    }
+}
+
+void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
+                          const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
+                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st)
+{
+    if (dim == 3) {
+        if (vf) k_accd_pipeline<3, true><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+        else k_accd_pipeline<3, false><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+    } else {
+        k_accd_pipeline<2, true><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+    }
+}
+
+void launch_accd_bulk(int dim, const int *sten, const unsigned char *is_vf, long long n, const double *V0,
+                      const double *V1, int nv, double vf_eta, double ee_eta, double *out_toi, int *out_hit,
+                      Counters *cnt, cudaStream_t st)
+{
+    if (n <= 0) return;
+    long long g = (n + 127) / 128;
+    if (g > 148 * 32) g = 148 * 32;
+    if (dim == 3) k_accd_bulk<3><<<(int)g, 128, 0, st>>>(sten, is_vf, n, V0, V1, nv, vf_eta, ee_eta, out_toi, out_hit, cnt);
+    else k_accd_bulk<2><<<(int)g, 128, 0, st>>>(sten, is_vf, n, V0, V1, nv, vf_eta, ee_eta, out_toi, out_hit, cnt);
+}
+
+} // namespace mclccd

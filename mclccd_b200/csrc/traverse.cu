@@ -1,0 +1,243 @@
+// Self-traversal of the LBVH and leaf-pair expansion.
+//
+// Replaces BVHTree::traverse/collide/get_candidates/default_discrete_test
+// (BVHTree.cpp:129-302, 305-398, 464-500).  The reference enumerates each
+// unordered pair of distinct leaves whose boxes pass boxes_intersect exactly
+// once (one frontlist seed per internal node, BVHTree.cpp:169-185); here each
+// sorted leaf q walks the tree for leaves k > q, so every unordered pair is
+// found once.  Inner nodes are tested with outward-rounded FP32 boxes (a
+// superset), leaves with the exact FP64 predicate, so the leaf-pair set is
+// exactly the reference's.  Pairs are emitted canonically (lower primitive
+// index first).
+#include "common.cuh"
+#include "geom.cuh"
+#include "kernels.cuh"
+
+namespace mclccd {
+
+constexpr int kStackDepth = 64;
+
+template <int DIM>
+__device__ __forceinline__ void child_boxes(const Node &N, float *llo, float *lhi, float *rlo, float *rhi)
+{
+    if constexpr (DIM == 3) {
+        llo[0] = N.a.x; llo[1] = N.a.y; llo[2] = N.a.z; lhi[0] = N.a.w; lhi[1] = N.b.x; lhi[2] = N.b.y;
+        rlo[0] = N.b.z; rlo[1] = N.b.w; rlo[2] = N.c.x; rhi[0] = N.c.y; rhi[1] = N.c.z; rhi[2] = N.c.w;
+    } else {
+        llo[0] = N.a.x; llo[1] = N.a.y; lhi[0] = N.a.z; lhi[1] = N.a.w;
+        rlo[0] = N.b.x; rlo[1] = N.b.y; rhi[0] = N.b.z; rhi[1] = N.b.w;
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ bool overlap32(const float *alo, const float *ahi, const float *blo, const float *bhi)
+{
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) ok = ok && (alo[k] <= bhi[k]) && (blo[k] <= ahi[k]);
+    return ok;
+}
+
+template <int DIM>
+__device__ __forceinline__ Node load_node(const Node *__restrict__ nodes, int i)
+{
+    Node N;
+    N.a = __ldg(&nodes[i].a);
+    N.b = __ldg(&nodes[i].b);
+    if constexpr (DIM == 3) N.c = __ldg(&nodes[i].c);
+    N.d = __ldg(&nodes[i].d);
+    return N;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128)
+k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
+           const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
+           int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n - 1) return;
+    const LeafBox<DIM> qb = leaf_box[q];
+    const bool qact = leaf_active[q] != 0;
+    const int qprim = sorted[q];
+    float qlo[DIM], qhi[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        qlo[k] = __double2float_rd(qb.lo0[k] < qb.lo1[k] ? qb.lo0[k] : qb.lo1[k]);
+        qhi[k] = __double2float_ru(qb.hi0[k] < qb.hi1[k] ? qb.hi1[k] : qb.hi0[k]);
+    }
+
+    auto exact = [&](int k) {
+        const LeafBox<DIM> kb = leaf_box[k];
+        if (leaf_boxes_intersect<DIM>(qb, kb)) {
+            const int kprim = __ldg(sorted + k);
+            unsigned long long slot = warp_append(&cnt->n_pairs);
+            if (slot < cap) pairs[slot] = make_int2(min(qprim, kprim), max(qprim, kprim));
+        }
+    };
+
+    int stack[kStackDepth];
+    int sp = 0;
+    int node = 0;
+    // A query visits each internal node at most once: n - 1 steps bound it.
+    for (int steps = 0;; ++steps) {
+        if (steps >= n) { atomicOr(&cnt->err, kErrStack); break; }
+        const Node N = load_node<DIM>(nodes, node);
+        const int split = N.d.x, meta = N.d.y, last = N.d.z;
+        float llo[DIM], lhi[DIM], rlo[DIM], rhi[DIM];
+        child_boxes<DIM>(N, llo, lhi, rlo, rhi);
+        const bool lact = ((meta >> 8) & 0xff) != 0, ract = ((meta >> 16) & 0xff) != 0;
+        bool lok = split > q && (qact || lact) && overlap32<DIM>(qlo, qhi, llo, lhi);
+        bool rok = last > q && (qact || ract) && overlap32<DIM>(qlo, qhi, rlo, rhi);
+        if (lok && (meta & kMetaLeftLeaf)) { exact(split); lok = false; }
+        if (rok && (meta & kMetaRightLeaf)) { exact(split + 1); rok = false; }
+        if (lok) {
+            if (rok) {
+                if (sp < kStackDepth) stack[sp++] = split + 1;
+                else atomicOr(&cnt->err, kErrStack);
+            }
+            node = split;
+        } else if (rok) {
+            node = split + 1;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Leaf pairs -> VF/EE stencils (get_candidates, BVHTree.cpp:305-398, with the
+// lower primitive as "left") and the discrete test at V1
+// (default_discrete_test, BVHTree.cpp:464-500).
+// Stencil bits: VF a->b slot i = bit i, VF b->a slot i = bit 3+i,
+// EE (i,j) = bit 6 + 3i + j.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ unsigned stencil_bits(const int *fa, const int *fb, unsigned ga, unsigned gb)
+{
+    unsigned bits = 0;
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) {
+        bool sa = false, sb = false;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) { sa |= fa[i] == fb[j]; sb |= fb[i] == fa[j]; }
+        if ((ga & (kFlagV0 << i)) && !sa) bits |= 1u << i;
+        if ((gb & (kFlagV0 << i)) && !sb) bits |= 1u << (3 + i);
+    }
+    if constexpr (DIM == 3) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            if (!(ga & (kFlagE0 << i))) continue;
+            const int a = fa[i], b = fa[(i + 1) % 3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                if (!(gb & (kFlagE0 << j))) continue;
+                const int c = fb[j], d = fb[(j + 1) % 3];
+                if (a == c || a == d || b == c || b == d) continue;
+                bits |= 1u << (6 + 3 * i + j);
+            }
+        }
+    }
+    return bits;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, const int *__restrict__ P,
+               const unsigned char *__restrict__ flags, const double *__restrict__ V1, int nv,
+               int4 *__restrict__ vf, unsigned long long vf_cap, int4 *__restrict__ ee, unsigned long long ee_cap,
+               int2 *__restrict__ disc, unsigned long long disc_cap, int continuous, int discrete, Counters *cnt)
+{
+    unsigned long long n = *(volatile unsigned long long *)&cnt->n_pairs;
+    if (n > pair_cap) n = pair_cap;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const unsigned long long idx = base + threadIdx.x;
+        const bool valid = idx < n;
+        int2 pr = make_int2(0, 0);
+        int fa[DIM], fb[DIM];
+        unsigned bits = 0;
+        if (valid) {
+            pr = pairs[idx];
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) { fa[k] = __ldg(P + (size_t)pr.x * DIM + k); fb[k] = __ldg(P + (size_t)pr.y * DIM + k); }
+            if (continuous) bits = stencil_bits<DIM>(fa, fb, __ldg(flags + pr.x), __ldg(flags + pr.y));
+        }
+        if (continuous) {
+            const unsigned nvf = __popc(bits & 0x3fu), nee = __popc(bits >> 6);
+            unsigned long long bvf = warp_reserve(&cnt->n_vf, nvf);
+            unsigned long long bee = DIM == 3 ? warp_reserve(&cnt->n_ee, nee) : 0ull;
+            for (unsigned m = bits & 0x3fu; m; m &= m - 1) {
+                const int b = __ffs(m) - 1;
+                const int *vs = b < 3 ? fa : fb;
+                const int *fs = b < 3 ? fb : fa;
+                if (bvf < vf_cap) vf[bvf] = make_int4(vs[b % 3], fs[0], fs[1], DIM == 3 ? fs[DIM - 1] : -1);
+                ++bvf;
+            }
+            if constexpr (DIM == 3) {
+                for (unsigned m = bits >> 6; m; m &= m - 1) {
+                    const int b = __ffs(m) - 1, i = b / 3, j = b % 3;
+                    if (bee < ee_cap) ee[bee] = make_int4(fa[i], fa[(i + 1) % 3], fb[j], fb[(j + 1) % 3]);
+                    ++bee;
+                }
+            }
+        }
+        if (discrete && valid) {
+            bool shared = false;
+#pragma unroll
+            for (int i = 0; i < DIM; ++i)
+#pragma unroll
+                for (int j = 0; j < DIM; ++j) shared |= fa[i] == fb[j];
+            bool inb = true;
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) inb = inb && fa[i] >= 0 && fa[i] < nv && fb[i] >= 0 && fb[i] < nv;
+            if (!inb) atomicOr(&cnt->err, kErrBadIndex);
+            int hit = 0;
+            if (!shared && inb) {
+                double A[DIM][DIM], B[DIM][DIM];
+#pragma unroll
+                for (int i = 0; i < DIM; ++i)
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) {
+                        A[i][k] = __ldg(V1 + (size_t)fa[i] * DIM + k);
+                        B[i][k] = __ldg(V1 + (size_t)fb[i] * DIM + k);
+                    }
+                if constexpr (DIM == 3) hit = tri_tri(A[0], A[1], A[2], B[0], B[1], B[2]);
+                else hit = seg_seg(A[0], A[1], B[0], B[1]);
+            }
+            if (hit) {
+                unsigned long long slot = warp_append(&cnt->n_discrete);
+                if (slot < disc_cap) disc[slot] = pr;
+            }
+        }
+    }
+}
+
+void launch_traverse(int dim, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
+                     const int *sorted, int n, int2 *pairs, unsigned long long cap, Counters *cnt, cudaStream_t st)
+{
+    if (n < 2) return;
+    const int g = (n - 1 + 127) / 128;
+    if (dim == 3)
+        k_traverse<3><<<g, 128, 0, st>>>(nodes, reinterpret_cast<const LeafBox<3> *>(leaf_box), leaf_active, sorted, n,
+                                         pairs, cap, cnt);
+    else
+        k_traverse<2><<<g, 128, 0, st>>>(nodes, reinterpret_cast<const LeafBox<2> *>(leaf_box), leaf_active, sorted, n,
+                                         pairs, cap, cnt);
+}
+
+void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,
+                         const unsigned char *flags, const double *V1, int nv, int4 *vf, unsigned long long vf_cap,
+                         int4 *ee, unsigned long long ee_cap, int2 *disc, unsigned long long disc_cap, int continuous,
+                         int discrete, Counters *cnt, int grid, cudaStream_t st)
+{
+    if (dim == 3)
+        k_expand_pairs<3><<<grid, 256, 0, st>>>(pairs, pair_cap, P, flags, V1, nv, vf, vf_cap, ee, ee_cap, disc,
+                                                disc_cap, continuous, discrete, cnt);
+    else
+        k_expand_pairs<2><<<grid, 256, 0, st>>>(pairs, pair_cap, P, flags, V1, nv, vf, vf_cap, ee, ee_cap, disc,
+                                                disc_cap, continuous, discrete, cnt);
+}
+
+} // namespace mclccd

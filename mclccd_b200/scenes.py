@@ -63,9 +63,14 @@ def folded_cloth(n: int = 64, seed: int = 0, fold_deg: float = 170.0,
     return np.ascontiguousarray(V0), np.ascontiguousarray(V1), F, eta
 
 
-def wavy_cloth(n: int = 1025, seed: int = 0, eta: float = 1e-4):
+def wavy_cloth(n: int = 1025, seed: int = 0, eta: float = 1e-4, rows: int | None = None):
+    """``rows`` < n keeps only the first ``rows`` grid rows (a strip of the
+    same cloth: same spacing, same motion field)."""
     h = 1.0 / (n - 1) if n == 1025 else 1.0 / 1024
     V, F = grid(n, h)
+    if rows is not None and rows < n:
+        V = V[: rows * n]
+        F = F[: 2 * (n - 1) * (rows - 1)]
     V0 = V.copy()
     V0[:, 2] = 0.05 * np.sin(8 * np.pi * V[:, 0]) * np.sin(8 * np.pi * V[:, 1])
     V1 = wavy_redraw(V0, seed, h)

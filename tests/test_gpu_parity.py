@@ -1,0 +1,230 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's golden
+fixtures and the oracle restatement on the same seeded inputs.
+
+Bar: leaf boxes, representative flags, the canonical candidate-stencil set,
+the discrete-pair set and hit/miss are bit-exact; toi is bit-exact too for the
+FP64 path (same IEEE operations, no FMA), tested at 0 ulp."""
+import os
+
+import numpy as np
+import pytest
+
+from mclccd_b200 import BVHTree, CCDError, narrow_phase_bulk, scenes
+from oracle.ref import Port, canonical_set, sort_rows
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+KATS = ["headon", "parallel", "shared", "static", "coplanar", "fold12", "spheres", "annulus48", "segments2d"]
+
+
+@pytest.fixture(scope="module")
+def port():
+    return Port()
+
+
+@pytest.fixture(scope="module")
+def kats():
+    z = np.load(os.path.join(GOLD, "kat_small.npz"))
+    return {name: {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(name + "/")} for name in z["names"]}
+
+
+def run_gpu(V0, V1, F, eta, **opts):
+    t = BVHTree(V0.shape[1])
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    for k, v in opts.items():
+        setattr(t.options, k, v)
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    return t
+
+
+def hit_map(sten, is_vf, toi):
+    return {(int(v),) + tuple(int(x) for x in s): float(t) for s, v, t in zip(sten, is_vf, toi)}
+
+
+def check_against_port(t, port, V0, V1, F, eta):
+    p = port.run(V0, V1, F, eta)
+    b, f = t.leaves(len(F))
+    assert np.array_equal(b, p["leaf_boxes"])
+    assert np.array_equal(f, p["leaf_flags"])
+    cs, cv = t.candidates()
+    assert np.array_equal(canonical_set(cs, cv), canonical_set(p["cand_sten"], p["cand_is_vf"]))
+    assert np.array_equal(sort_rows(t.discrete()), sort_rows(p["discrete"]))
+    hs, hv, ht = t.hits()
+    # same orientation convention as the port (lower primitive first): exact maps
+    got = hit_map(hs, hv, ht)
+    want = hit_map(p["hit_sten"], p["hit_is_vf"], p["hit_toi"])
+    assert got.keys() == want.keys()
+    bad = [k for k in want if got[k] != want[k]]
+    assert not bad, f"{len(bad)} toi mismatches, e.g. {bad[:3]}"
+    return p
+
+
+@pytest.mark.parametrize("name", KATS)
+def test_kat_against_reference_golden(kats, name):
+    g = kats[name]
+    eta = float(g["eta"])
+    t = run_gpu(g["V0"], g["V1"], g["F"], eta)
+    b, f = t.leaves(len(g["F"]))
+    assert np.array_equal(b, g["leaf_boxes"])
+    flags = np.stack([(f >> j) & 1 for j in range(7)], axis=1)
+    assert np.array_equal(flags, g["leaf_flags"])
+    cs, cv = t.candidates()
+    assert np.array_equal(canonical_set(cs, cv), g["cand"])
+    assert np.array_equal(sort_rows(t.discrete()), g["discrete"])
+    hs, hv, ht = t.hits()
+    assert np.array_equal(canonical_set(hs, hv), g["hits"])
+    want = hit_map(g["canon_sten"][g["canon_hit"] == 1], g["canon_is_vf"][g["canon_hit"] == 1],
+                   g["canon_toi"][g["canon_hit"] == 1])
+    assert hit_map(hs, hv, ht) == want
+
+
+def test_cfg0_folded_cloth(port):
+    V0, V1, F, eta = scenes.folded_cloth(64)
+    t = run_gpu(V0, V1, F, eta)
+    c = t.counts()
+    assert (c["vf"], c["ee"], c["hits"], c["discrete"]) == (768841, 1711130, 2410926, 1061)
+    check_against_port(t, port, V0, V1, F, eta)
+
+
+@pytest.mark.parametrize("scene", ["wavy129", "spheres", "annulus", "fold_big_motion"])
+def test_scenes_against_port(port, scene):
+    V0, V1, F, eta = {
+        "wavy129": lambda: scenes.wavy_cloth(129, seed=3),
+        "spheres": lambda: scenes.icospheres(12, 3, seed=5),
+        "annulus": lambda: scenes.annulus_2d(400, seed=7),
+        "fold_big_motion": lambda: scenes.folded_cloth(40, seed=9, noise=0.02),
+    }[scene]()
+    t = run_gpu(V0, V1, F, eta)
+    check_against_port(t, port, V0, V1, F, eta)
+
+
+def test_refit_equals_rebuild(port):
+    V0, V1, F, eta = scenes.wavy_cloth(97, seed=1)
+    V1b = scenes.wavy_redraw(V0, 77)
+    t = run_gpu(V0, V1, F, eta)
+    t.update(V0, V1b, F)            # same F -> refit-only path
+    t.traverse(V0, V1b, F)
+    check_against_port(t, port, V0, V1b, F, eta)
+    u = run_gpu(V0, V1b, F, eta, always_rebuild=True)
+    for a, b in ((t.candidates(), u.candidates()),):
+        assert np.array_equal(canonical_set(*a), canonical_set(*b))
+
+
+def test_options(port):
+    V0, V1, F, eta = scenes.folded_cloth(24, seed=4)
+    # continuous off: no stencils; discrete off: no discrete pairs
+    t = run_gpu(V0, V1, F, eta, continuous=False)
+    c = t.counts()
+    assert c["vf"] == c["ee"] == c["hits"] == 0 and c["discrete"] == len(port.run(V0, V1, F, eta)["discrete"])
+    t = run_gpu(V0, V1, F, eta, discrete=False)
+    assert t.counts()["discrete"] == 0
+    # reptri off: every vertex / edge slot represented (BVHLeaf.hpp:45-49)
+    t = run_gpu(V0, V1, F, eta, reptri=False)
+    p = port.run(V0, V1, F, eta, reptri=False)
+    cs, cv = t.candidates()
+    assert np.array_equal(canonical_set(cs, cv), canonical_set(p["cand_sten"], p["cand_is_vf"]))
+    # gaps above box_eta are clamped to it (BVHTree.cpp:39-40)
+    t = BVHTree(3)
+    t.options.box_eta, t.options.vf_ccd_eta, t.options.ee_ccd_eta = eta, 10 * eta, 10 * eta
+    t.update(V0, V1, F)
+    assert t.options.vf_ccd_eta == eta and t.options.ee_ccd_eta == eta
+    t.traverse(V0, V1, F)
+    q = port.run(V0, V1, F, eta)
+    assert np.array_equal(canonical_set(*t.hits()[:2]), canonical_set(q["hit_sten"], q["hit_is_vf"]))
+
+
+def test_active_mask(port):
+    V0, V1, F, eta = scenes.folded_cloth(24, seed=6)
+    rng = np.random.default_rng(0)
+    active = (rng.random(len(V0)) < 0.1).astype(np.int32)
+    t = BVHTree(3)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.update(V0, V1, F, active=active)
+    t.traverse(V0, V1, F)
+    p = port.run(V0, V1, F, eta, active=active)
+    cs, cv = t.candidates()
+    assert np.array_equal(canonical_set(cs, cv), canonical_set(p["cand_sten"], p["cand_is_vf"]))
+    b, f = t.leaves(len(F))
+    assert np.array_equal(f, p["leaf_flags"])
+
+
+def test_hooks_and_stop():
+    V0, V1, F, eta = scenes.folded_cloth(32, seed=2)
+    t = BVHTree(3)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    got, disc = [], []
+    t.append_pair = lambda s, v, toi: got.append((tuple(s), v, toi))
+    t.append_discrete = lambda a, b: (disc.append((a, b)), True)[1]   # stop after the first
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    c = t.counts()
+    assert len(got) == c["hits"] and all(toi >= 0 for _, _, toi in got)
+    assert len(disc) == (1 if c["discrete"] else 0)
+    # host filter_pair / narrow_phase hooks
+    t2 = BVHTree(3)
+    t2.options.box_eta = t2.options.vf_ccd_eta = t2.options.ee_ccd_eta = eta
+    t2.filter_pair = lambda s, is_vf: not is_vf          # keep VF only
+    t2.update(V0, V1, F)
+    t2.traverse(V0, V1, F)
+    hs, hv, ht = t2.hits()
+    full = t.hits()
+    assert np.all(hv == 1)
+    assert len(hs) == int(np.sum(full[1] == 1))
+
+
+def test_empty_single_and_errors():
+    V = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float64)
+    t = BVHTree(3)
+    t.update(V, V, np.zeros((0, 3), np.int32))
+    t.traverse(V, V, np.zeros((0, 3), np.int32))
+    assert t.counts()["hits"] == 0
+    t.update(V, V + 0.1, np.array([[0, 1, 2]], np.int32))
+    t.traverse(V, V + 0.1, np.array([[0, 1, 2]], np.int32))
+    assert t.counts()["leaf_pairs"] == 0
+    bad = BVHTree(3)
+    with pytest.raises(CCDError) as e:
+        bad.traverse(V, V, np.array([[0, 1, 2]], np.int32))
+    assert e.value.status == 5   # STATE: traverse before update
+    with pytest.raises(CCDError) as e:
+        bad.update(V, V, np.array([[0, 1, 7], [0, 1, 2]], np.int32))
+    assert e.value.status == 1   # index out of range
+    bad.options.vf_one_sided = True
+    with pytest.raises(CCDError) as e:
+        bad.update(V, V, np.array([[0, 1, 2]], np.int32))
+    assert e.value.status == 7
+
+
+def test_bulk_narrow_phase_matches_port(port):
+    rng = np.random.default_rng(3)
+    n, nv = 20000, 4000
+    V0 = rng.random((nv, 3))
+    V1 = V0 + rng.normal(0, 0.05, V0.shape)
+    sten = rng.integers(0, nv, (n, 4)).astype(np.int32)
+    is_vf = (rng.random(n) < 0.5).astype(np.uint8)
+    # degenerate stencils: repeated vertices, zero motion, parallel edges
+    sten[:200, 1] = sten[:200, 0]
+    V1[:50] = V0[:50]
+    sten[200:300, 2:] = sten[200:300, :2]
+    for eta in (1e-3, 0.05):
+        toi, hit = narrow_phase_bulk(V0, V1, sten, is_vf, eta)
+        h2, t2 = port.accd(V0, V1, sten, is_vf, eta)
+        assert np.array_equal(hit, h2)
+        assert np.array_equal(toi, t2)
+    z = np.load(os.path.join(GOLD, "cfg0_sample.npz"))
+    V0, V1, F, eta = scenes.folded_cloth(64)
+    toi, hit = narrow_phase_bulk(V0, V1, z["sten"], z["is_vf"], eta)
+    assert np.array_equal(hit, z["hit"]) and np.array_equal(toi, z["toi"])
+
+
+def test_device_tensors(port):
+    torch = pytest.importorskip("torch")
+    V0, V1, F, eta = scenes.folded_cloth(48, seed=8)
+    d = lambda a: torch.from_numpy(a).cuda()
+    t = BVHTree(3)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.update(d(V0), d(V1), d(F))
+    t.traverse(d(V0), d(V1), d(F))
+    check_against_port(t, port, V0, V1, F, eta)
+    t.traverse()   # NULL arrays: reuse the update's
+    check_against_port(t, port, V0, V1, F, eta)
