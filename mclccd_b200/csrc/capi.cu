@@ -20,7 +20,7 @@ struct DevBuf {
 
 constexpr int kExpandGrid = 148 * 8;
 constexpr int kAccdGrid = 148 * 16;
-constexpr int kMaxAttempts = 3;
+constexpr int kMaxAttempts = 6;
 
 struct DeviceGuard {
     int prev = -1;
@@ -448,14 +448,18 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
         MC_CUDA(t, cudaStreamSynchronize(st));
         const Counters &c = *t->h_cnt;
         bool grow = false;
-        auto need = [&](unsigned long long count, unsigned long long &cap) {
-            if (count > cap) { cap = count + count / 4 + 1024; grow = true; }
+        auto need = [&](double count, unsigned long long &cap) {
+            if (count > (double)cap) { cap = (unsigned long long)(count * 1.25) + 1024; grow = true; }
         };
-        need(c.n_pairs, t->cap_pairs);
-        need(c.n_vf, t->cap_vf);
-        need(c.n_ee, t->cap_ee);
-        need(c.n_hits, t->cap_hits);
-        need(c.n_discrete, t->cap_disc);
+        // Stencil and discrete counts only cover the leaf pairs that fit; scale
+        // them by the leaf-pair shortfall so one regrow usually suffices.
+        const double r = c.n_pairs > t->cap_pairs ? (double)c.n_pairs / (double)t->cap_pairs : 1.0;
+        need((double)c.n_pairs, t->cap_pairs);
+        need(r * (double)c.n_vf, t->cap_vf);
+        need(r * (double)c.n_ee, t->cap_ee);
+        need(r * (double)c.n_discrete, t->cap_disc);
+        // A hit is a candidate: this capacity never overflows on its own.
+        t->cap_hits = std::max(t->cap_hits, t->cap_vf + t->cap_ee);
         if (!grow) break;
         if (attempt + 1 >= kMaxAttempts) return fail(t, MCLCCD_ERR_DEVICE, "result buffers kept overflowing");
     }

@@ -49,7 +49,9 @@ k_accd_pipeline(const int4 *__restrict__ sten, const unsigned long long *n_ptr, 
         int iters;
         const int hit = accd<DIM, VF>(x0, x1, eta, toi, iters);
         if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
-        if (hit) {
+        // collide() delivers a hit only when toi >= 0 (BVHTree.cpp:262): a
+        // degenerate stencil can report hit == 1 with toi = NaN.
+        if (hit && toi >= 0.0) {
             const unsigned long long slot = warp_append(&cnt->n_hits);
             if (slot < hit_cap) {
                 hit_sten[slot] = s4;

@@ -235,7 +235,7 @@ class Port:
         if continuous:
             cs, cv = self.candidates(F, flags, pairs)
             hit, toi = self.accd(V0, V1, cs, cv, vf_eta, ee_eta)
-            m = hit == 1
+            m = (hit == 1) & (toi >= 0)   # collide() delivers only toi >= 0 (BVHTree.cpp:262)
             out.update(cand_sten=cs, cand_is_vf=cv, hit_sten=cs[m], hit_is_vf=cv[m], hit_toi=toi[m])
         else:
             e = np.zeros((0, 4), np.int32)

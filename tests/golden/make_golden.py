@@ -59,6 +59,12 @@ def kat_scenes():
     V0 = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0.2, 0.2, 0.3], [1.2, 0.2, 0.3], [0.2, 1.2, 0.3]])
     V1 = V0.copy(); V1[3:, 2] = 0.0
     out.append(("coplanar", V0, V1, np.array([[0, 1, 2], [3, 4, 5]], np.int32), 1e-3))
+    # Degenerate triangle (repeated vertex) sweeping through another: its VF
+    # stencils have NaN distance, ACCD reports hit with toi = NaN, and
+    # collide() drops them (toi >= 0 gate, BVHTree.cpp:262).
+    V0 = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0.2, 0.2, 0.1], [0.3, 0.25, 0.1]], np.float64)
+    V1 = V0.copy(); V1[3:, 2] = -0.1
+    out.append(("degenerate", V0, V1, np.array([[0, 1, 2], [3, 4, 4]], np.int32), 1e-3))
     out.append(("fold12", *scenes.folded_cloth(12, seed=5)))
     out.append(("spheres", *scenes.icospheres(3, 2, seed=4)))
     out.append(("annulus48", *scenes.annulus_2d(48, seed=2)))

@@ -30,11 +30,11 @@ def _flags_bits(pf):
 
 
 def test_kat_scenes_present(kats):
-    assert {"headon", "parallel", "shared", "static", "coplanar", "fold12", "spheres", "annulus48",
+    assert {"headon", "parallel", "shared", "static", "coplanar", "degenerate", "fold12", "spheres", "annulus48",
             "segments2d"} <= set(kats)
 
 
-@pytest.mark.parametrize("name", ["headon", "parallel", "shared", "static", "coplanar", "fold12", "spheres",
+@pytest.mark.parametrize("name", ["headon", "parallel", "shared", "static", "coplanar", "degenerate", "fold12", "spheres",
                                   "annulus48", "segments2d"])
 def test_port_matches_reference_golden(port, kats, name):
     g = kats[name]
@@ -47,7 +47,7 @@ def test_port_matches_reference_golden(port, kats, name):
     assert np.array_equal(canonical_set(p["hit_sten"], p["hit_is_vf"]), g["hits"])
     hit, toi = port.accd(g["V0"], g["V1"], g["canon_sten"], g["canon_is_vf"], eta)
     assert np.array_equal(hit, g["canon_hit"])
-    assert np.array_equal(toi, g["canon_toi"])                              # bit-exact toi
+    assert np.array_equal(toi, g["canon_toi"], equal_nan=True)              # bit-exact toi (NaN: degenerate)
 
 
 def test_shared_vertex_and_static_semantics(kats):
