@@ -475,9 +475,12 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
     t->n_ee = c.n_ee;
     t->n_hits = c.n_hits;
     t->n_disc = c.n_discrete;
-    if (c.err) {
+    // kErrAccdIters only notes that some stencil ran ACCD's full 1000
+    // iterations (the reference then reports a hit too); it is not a failure.
+    const unsigned fatal = c.err & ~kErrAccdIters;
+    if (fatal) {
         t->traversed = false;
-        return device_errors(t, c.err);
+        return device_errors(t, fatal);
     }
     return MCLCCD_OK;
 }
