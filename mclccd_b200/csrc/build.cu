@@ -180,46 +180,48 @@ __global__ void k_karras(const unsigned *__restrict__ keys, int n, Node *__restr
 // ---------------------------------------------------------------------------
 // Refit: one thread per sorted leaf computes the exact FP64 leaf box (stored
 // in sorted order for the traversal's exact test) and its outward-rounded
-// FP32 swept box, writes it into the parent's child slot, then climbs: the
-// second thread to reach an internal node merges both child slots and moves
-// up (first arrival stops).  `visits` must be zero on entry.
+// FP32 t0 and t1 boxes, writes them into the parent's child slot, then
+// climbs: the second thread to reach an internal node merges both child slots
+// and moves up (first arrival stops).  `visits` must be zero on entry.
 // ---------------------------------------------------------------------------
 template <int DIM>
-__device__ __forceinline__ void write_child(Node *nodes, int parent, bool right, const float *lo, const float *hi, bool act)
+__device__ __forceinline__ void write_child(Node *nodes, int parent, bool right, const Box2T<DIM> &b, bool act)
 {
     Node *nd = nodes + parent;
-    if constexpr (DIM == 3) {
-        // Children of one parent share float4 b: the two writers are serialised
-        // by the refit protocol only for reads, so split b by 8-byte halves.
-        float2 *b2 = reinterpret_cast<float2 *>(&nd->b);
-        if (!right) {
-            nd->a = make_float4(lo[0], lo[1], lo[2], hi[0]);
-            b2[0] = make_float2(hi[1], hi[2]);
-        } else {
-            b2[1] = make_float2(lo[0], lo[1]);
-            nd->c = make_float4(lo[2], hi[0], hi[1], hi[2]);
-        }
-    } else {
-        if (!right) nd->a = make_float4(lo[0], lo[1], hi[0], hi[1]);
-        else nd->b = make_float4(lo[0], lo[1], hi[0], hi[1]);
-    }
+    pack_child<DIM>(right ? nd->r : nd->l, b);
     reinterpret_cast<unsigned char *>(&nd->d.y)[right ? 2 : 1] = act ? 1 : 0;
 }
 
 template <int DIM>
-__device__ __forceinline__ void read_children(const Node *nd, float *lo, float *hi, bool &act)
+__device__ __forceinline__ void merge_children(const Node *nd, Box2T<DIM> &out, bool &act)
 {
-    float4 a = __ldcg(&nd->a), b = __ldcg(&nd->b);
-    int meta = __ldcg(&nd->d.y);
+    constexpr int S = DIM == 3 ? 3 : 2;
+    float4 ls[S], rs[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) { ls[i] = __ldcg(&nd->l[i]); rs[i] = __ldcg(&nd->r[i]); }
+    const int meta = __ldcg(&nd->d.y);
     act = ((meta >> 8) & 0xff) || ((meta >> 16) & 0xff);
-    if constexpr (DIM == 3) {
-        float4 c = __ldcg(&nd->c);
-        lo[0] = fminf(a.x, b.z); lo[1] = fminf(a.y, b.w); lo[2] = fminf(a.z, c.x);
-        hi[0] = fmaxf(a.w, c.y); hi[1] = fmaxf(b.x, c.z); hi[2] = fmaxf(b.y, c.w);
-    } else {
-        lo[0] = fminf(a.x, b.x); lo[1] = fminf(a.y, b.y);
-        hi[0] = fmaxf(a.z, b.z); hi[1] = fmaxf(a.w, b.w);
+    Box2T<DIM> a, b;
+    unpack_child<DIM>(ls, a);
+    unpack_child<DIM>(rs, b);
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        out.t0lo[k] = fminf(a.t0lo[k], b.t0lo[k]); out.t0hi[k] = fmaxf(a.t0hi[k], b.t0hi[k]);
+        out.t1lo[k] = fminf(a.t1lo[k], b.t1lo[k]); out.t1hi[k] = fmaxf(a.t1hi[k], b.t1hi[k]);
     }
+}
+
+// FP32 boxes that contain the FP64 ones (round min down, max up).
+template <int DIM>
+__device__ __forceinline__ Box2T<DIM> outward(const LeafBox<DIM> &b)
+{
+    Box2T<DIM> o;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        o.t0lo[k] = __double2float_rd(b.lo0[k]); o.t0hi[k] = __double2float_ru(b.hi0[k]);
+        o.t1lo[k] = __double2float_rd(b.lo1[k]); o.t1hi[k] = __double2float_ru(b.hi1[k]);
+    }
+    return o;
 }
 
 template <int DIM>
@@ -238,27 +240,22 @@ __global__ void k_refit(const double *__restrict__ V0, const double *__restrict_
     leaf_box[k] = b;
     leaf_active[k] = act ? 1 : 0;
     if (np < 2) return;
-    float lo[DIM], hi[DIM];
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-        lo[c] = __double2float_rd(b.lo0[c] < b.lo1[c] ? b.lo0[c] : b.lo1[c]);
-        hi[c] = __double2float_ru(b.hi0[c] < b.hi1[c] ? b.hi1[c] : b.hi0[c]);
-    }
+    Box2T<DIM> box = outward<DIM>(b);
     int parent = leaf_parent[k];
     bool right = __ldg(&nodes[parent].d.x) != k;
-    write_child<DIM>(nodes, parent, right, lo, hi, act);
+    write_child<DIM>(nodes, parent, right, box, act);
     for (int level = 0; level < 256; ++level) {   // depth of a Karras tree over 30-bit keys is < 64
         __threadfence();
         if (atomicAdd(visits + parent, 1) == 0) return;   // sibling subtree not done yet
         __threadfence();
         const int node = parent;
-        read_children<DIM>(nodes + node, lo, hi, act);
+        merge_children<DIM>(nodes + node, box, act);
         parent = __ldcg(&nodes[node].d.w);
         if (parent < 0) return;   // root: its own box is never needed
         const int psplit = __ldg(&nodes[parent].d.x);
         const int pmeta = __ldg(&nodes[parent].d.y) & 0xff;
         right = !(psplit == node && !(pmeta & kMetaLeftLeaf));
-        write_child<DIM>(nodes, parent, right, lo, hi, act);
+        write_child<DIM>(nodes, parent, right, box, act);
     }
     atomicOr(&cnt->err, kErrStack);
 }

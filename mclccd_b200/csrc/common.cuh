@@ -40,19 +40,73 @@ struct Counters {
 // ---------------------------------------------------------------------------
 // Hierarchy layout (LBVH, Karras 2012).  Internal node i has children
 // split and split+1; each child is a leaf (sorted position) or an internal
-// node.  The children's FP32 swept boxes live in the parent, so one 64-byte
-// node read tests both children.
-//   3D: a = (lo_l.x, lo_l.y, lo_l.z, hi_l.x)  b = (hi_l.y, hi_l.z, lo_r.x, lo_r.y)
-//       c = (lo_r.z, hi_r.x, hi_r.y, hi_r.z)
-//   2D: a = (lo_l.x, lo_l.y, hi_l.x, hi_l.y)  b = (lo_r.x, lo_r.y, hi_r.x, hi_r.y)
+// node.  Each child's FP32 t0 box and t1 box (outward-rounded; unions for
+// inner nodes) live in the parent, so one 128-byte node read applies the
+// reference's whole box predicate -- swept overlap and the t0/t1 same-side
+// separation test -- to both children.
+//   3D child (3 x float4): (t0lo.x t0lo.y t0lo.z t0hi.x) (t0hi.y t0hi.z t1lo.x t1lo.y)
+//                          (t1lo.z t1hi.x t1hi.y t1hi.z)
+//   2D child (2 x float4): (t0lo.x t0lo.y t0hi.x t0hi.y) (t1lo.x t1lo.y t1hi.x t1hi.y)
 //   d = (split, meta, last, parent)
 // meta byte 0: bit0 left child is a leaf, bit1 right child is a leaf;
 // byte 1: left child active; byte 2: right child active.
 // ---------------------------------------------------------------------------
 struct __align__(16) Node {
-    float4 a, b, c;
+    float4 l[3];
+    float4 r[3];
     int4 d;
+    int4 pad;
 };
+
+// FP32 t0/t1 boxes of one child or query.
+template <int DIM>
+struct Box2T {
+    float t0lo[DIM], t0hi[DIM], t1lo[DIM], t1hi[DIM];
+};
+
+template <int DIM>
+__device__ __forceinline__ void unpack_child(const float4 *s, Box2T<DIM> &b)
+{
+    if constexpr (DIM == 3) {
+        b.t0lo[0] = s[0].x; b.t0lo[1] = s[0].y; b.t0lo[2] = s[0].z; b.t0hi[0] = s[0].w;
+        b.t0hi[1] = s[1].x; b.t0hi[2] = s[1].y; b.t1lo[0] = s[1].z; b.t1lo[1] = s[1].w;
+        b.t1lo[2] = s[2].x; b.t1hi[0] = s[2].y; b.t1hi[1] = s[2].z; b.t1hi[2] = s[2].w;
+    } else {
+        b.t0lo[0] = s[0].x; b.t0lo[1] = s[0].y; b.t0hi[0] = s[0].z; b.t0hi[1] = s[0].w;
+        b.t1lo[0] = s[1].x; b.t1lo[1] = s[1].y; b.t1hi[0] = s[1].z; b.t1hi[1] = s[1].w;
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ void pack_child(float4 *s, const Box2T<DIM> &b)
+{
+    if constexpr (DIM == 3) {
+        s[0] = make_float4(b.t0lo[0], b.t0lo[1], b.t0lo[2], b.t0hi[0]);
+        s[1] = make_float4(b.t0hi[1], b.t0hi[2], b.t1lo[0], b.t1lo[1]);
+        s[2] = make_float4(b.t1lo[2], b.t1hi[0], b.t1hi[1], b.t1hi[2]);
+    } else {
+        s[0] = make_float4(b.t0lo[0], b.t0lo[1], b.t0hi[0], b.t0hi[1]);
+        s[1] = make_float4(b.t1lo[0], b.t1lo[1], b.t1hi[0], b.t1hi[1]);
+    }
+}
+
+// The reference's box predicate (BVHTree.cpp:401-426, without the active
+// test) on FP32 boxes.  With outward-rounded leaf boxes and exact unions it
+// never rejects a pair the FP64 predicate accepts.
+template <int DIM>
+__device__ __forceinline__ bool boxes_may_intersect(const Box2T<DIM> &q, const Box2T<DIM> &c)
+{
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        const float qlo = fminf(q.t0lo[k], q.t1lo[k]), qhi = fmaxf(q.t0hi[k], q.t1hi[k]);
+        const float clo = fminf(c.t0lo[k], c.t1lo[k]), chi = fmaxf(c.t0hi[k], c.t1hi[k]);
+        ok = ok && clo <= qhi && qlo <= chi;
+        ok = ok && !((c.t0lo[k] > q.t0hi[k] && c.t1lo[k] > q.t1hi[k]) ||
+                     (c.t0hi[k] < q.t0lo[k] && c.t1hi[k] < q.t1lo[k]));
+    }
+    return ok;
+}
 constexpr int kMetaLeftLeaf = 1;
 constexpr int kMetaRightLeaf = 2;
 

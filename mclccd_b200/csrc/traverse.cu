@@ -18,53 +18,22 @@ namespace mclccd {
 constexpr int kStackDepth = 64;
 
 template <int DIM>
-__device__ __forceinline__ void child_boxes(const Node &N, float *llo, float *lhi, float *rlo, float *rhi)
-{
-    if constexpr (DIM == 3) {
-        llo[0] = N.a.x; llo[1] = N.a.y; llo[2] = N.a.z; lhi[0] = N.a.w; lhi[1] = N.b.x; lhi[2] = N.b.y;
-        rlo[0] = N.b.z; rlo[1] = N.b.w; rlo[2] = N.c.x; rhi[0] = N.c.y; rhi[1] = N.c.z; rhi[2] = N.c.w;
-    } else {
-        llo[0] = N.a.x; llo[1] = N.a.y; lhi[0] = N.a.z; lhi[1] = N.a.w;
-        rlo[0] = N.b.x; rlo[1] = N.b.y; rhi[0] = N.b.z; rhi[1] = N.b.w;
-    }
-}
-
-template <int DIM>
-__device__ __forceinline__ bool overlap32(const float *alo, const float *ahi, const float *blo, const float *bhi)
-{
-    bool ok = true;
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) ok = ok && (alo[k] <= bhi[k]) && (blo[k] <= ahi[k]);
-    return ok;
-}
-
-template <int DIM>
-__device__ __forceinline__ Node load_node(const Node *__restrict__ nodes, int i)
-{
-    Node N;
-    N.a = __ldg(&nodes[i].a);
-    N.b = __ldg(&nodes[i].b);
-    if constexpr (DIM == 3) N.c = __ldg(&nodes[i].c);
-    N.d = __ldg(&nodes[i].d);
-    return N;
-}
-
-template <int DIM>
 __global__ void __launch_bounds__(128)
 k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
            const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
            int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
 {
+    constexpr int S = DIM == 3 ? 3 : 2;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n - 1) return;
     const LeafBox<DIM> qb = leaf_box[q];
     const bool qact = leaf_active[q] != 0;
     const int qprim = sorted[q];
-    float qlo[DIM], qhi[DIM];
+    Box2T<DIM> qbox;
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
-        qlo[k] = __double2float_rd(qb.lo0[k] < qb.lo1[k] ? qb.lo0[k] : qb.lo1[k]);
-        qhi[k] = __double2float_ru(qb.hi0[k] < qb.hi1[k] ? qb.hi1[k] : qb.hi0[k]);
+        qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
+        qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
     }
 
     auto exact = [&](int k) {
@@ -76,24 +45,30 @@ k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf
         }
     };
 
-    int stack[kStackDepth];
+    // Per-thread stack in shared memory, [depth][thread]: conflict-free.
+    __shared__ int stack[kStackDepth][128];
+    const int tid = threadIdx.x;
     int sp = 0;
     int node = 0;
     // A query visits each internal node at most once: n - 1 steps bound it.
     for (int steps = 0;; ++steps) {
         if (steps >= n) { atomicOr(&cnt->err, kErrStack); break; }
-        const Node N = load_node<DIM>(nodes, node);
-        const int split = N.d.x, meta = N.d.y, last = N.d.z;
-        float llo[DIM], lhi[DIM], rlo[DIM], rhi[DIM];
-        child_boxes<DIM>(N, llo, lhi, rlo, rhi);
+        float4 ls[S], rs[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) { ls[i] = __ldg(&nodes[node].l[i]); rs[i] = __ldg(&nodes[node].r[i]); }
+        const int4 d = __ldg(&nodes[node].d);
+        const int split = d.x, meta = d.y, last = d.z;
+        Box2T<DIM> lb, rb;
+        unpack_child<DIM>(ls, lb);
+        unpack_child<DIM>(rs, rb);
         const bool lact = ((meta >> 8) & 0xff) != 0, ract = ((meta >> 16) & 0xff) != 0;
-        bool lok = split > q && (qact || lact) && overlap32<DIM>(qlo, qhi, llo, lhi);
-        bool rok = last > q && (qact || ract) && overlap32<DIM>(qlo, qhi, rlo, rhi);
+        bool lok = split > q && (qact || lact) && boxes_may_intersect<DIM>(qbox, lb);
+        bool rok = last > q && (qact || ract) && boxes_may_intersect<DIM>(qbox, rb);
         if (lok && (meta & kMetaLeftLeaf)) { exact(split); lok = false; }
         if (rok && (meta & kMetaRightLeaf)) { exact(split + 1); rok = false; }
         if (lok) {
             if (rok) {
-                if (sp < kStackDepth) stack[sp++] = split + 1;
+                if (sp < kStackDepth) stack[sp++][tid] = split + 1;
                 else atomicOr(&cnt->err, kErrStack);
             }
             node = split;
@@ -101,7 +76,7 @@ k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf
             node = split + 1;
         } else {
             if (sp == 0) break;
-            node = stack[--sp];
+            node = stack[--sp][tid];
         }
     }
 }
