@@ -1,0 +1,247 @@
+// Drop-in C++ replacement for mclccd's mcl::BVHTree<double, DIM>
+// (include/MCL/BVHTree.hpp), running the CCD path on the GPU through the C ABI
+// in include/mclccd_b200.h.  Link with libmclccd_b200.so.
+//
+// Same members as the reference: Options (same fields and defaults),
+// update(), traverse(), and the hooks append_pair, append_discrete,
+// filter_pair and narrow_phase.  After traverse() the hooks are called from
+// the calling thread, fed from the device result buffers:
+//   * append_pair(sten, is_vf, toi) once per CCD hit (toi >= 0);
+//   * append_discrete(p0, p1) once per discrete pair until it returns true;
+//   * filter_pair / narrow_phase, when set, are applied on the host to the
+//     candidate stencils (the default device ACCD scores the survivors when
+//     only filter_pair is set).
+// EE stencils and discrete pairs come with the lower primitive index first.
+// Errors throw mcl::CCDError (the reference asserts or silently returns).
+#pragma once
+
+#include "../mclccd_b200.h"
+
+#include <algorithm>
+#include <array>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#if defined(__has_include)
+#if __has_include(<Eigen/Core>)
+#include <Eigen/Core>
+#define MCLCCD_B200_HAVE_EIGEN 1
+#endif
+#endif
+
+namespace mcl {
+
+#ifdef MCLCCD_B200_HAVE_EIGEN
+typedef Eigen::Vector4i Stencil;
+#else
+typedef std::array<int, 4> Stencil;
+#endif
+
+class CCDError : public std::runtime_error {
+public:
+    CCDError(int status, const std::string &msg) : std::runtime_error(msg), status(status) {}
+    int status;
+};
+
+template <typename T, int DIM>
+class BVHTree;
+
+template <int DIM>
+class BVHTree<double, DIM> {
+    static_assert(DIM == 2 || DIM == 3, "mcl::BVHTree<double, DIM>: DIM must be 2 or 3");
+
+public:
+    struct Options {
+        double box_eta = 1e-6;     // padding of tree boxes
+        double vf_ccd_eta = 1e-6;  // gap for vf narrowphase <= box_eta
+        double ee_ccd_eta = 1e-6;  // gap for ee narrowphase <= box_eta
+        bool reptri = true;        // representative triangles
+        bool threaded = true;      // accepted; the GPU path is always parallel
+        bool discrete = true;      // discrete check ff/ee at V1
+        bool continuous = true;    // ccd check from V0 to V1
+        bool vf_one_sided = false; // CTCD narrow phase: not provided (throws)
+        bool ee_robust = true;     // unused by ACCD, as in the reference
+    } options;
+
+    std::function<void(const Stencil &sten, bool is_vf, const double &toi)> append_pair;
+    std::function<bool(int p0, int p1)> append_discrete;
+    std::function<bool(const Stencil &sten, bool is_vf)> filter_pair;
+    std::function<double(const Stencil &sten, bool is_vf)> narrow_phase;
+
+    BVHTree() { check(mclccd_create(DIM, &h_)); }
+    ~BVHTree() { if (h_) mclccd_destroy(h_); }
+    BVHTree(const BVHTree &) = delete;
+    BVHTree &operator=(const BVHTree &) = delete;
+
+    // Reference signature (BVHTree.hpp:81-82).  It carries no vertex count, so
+    // the count is taken as 1 + the largest index in P.
+    void update(const double *V0, const double *V1, const int *P, int np, int pdim, const int *active = nullptr)
+    {
+        int nv = 0;
+        for (long long i = 0; i < (long long)np * pdim; ++i) nv = std::max(nv, P[i] + 1);
+        update(V0, V1, nv, P, np, pdim, active, MCLCCD_MEM_HOST);
+    }
+
+    // With an explicit vertex count; mem_kind MCLCCD_MEM_DEVICE takes device
+    // pointers (no host copies at all).
+    void update(const double *V0, const double *V1, int nv, const int *P, int np, int pdim, const int *active,
+                int mem_kind)
+    {
+        push_options();
+        int rc = mclccd_update(h_, V0, V1, nv, P, np, pdim, active, mem_kind);
+        pull_options();
+        check(rc);
+        nv_ = nv;
+        np_ = np;
+        mem_ = mem_kind;
+    }
+
+    // Reference signature (BVHTree.hpp:86).  Runs the device pipeline on the
+    // given arrays (same side as the last update), then calls the hooks.
+    void traverse(const double *V0, const double *V1, const int *P) const
+    {
+        auto *self = const_cast<BVHTree *>(this);
+        self->push_options();
+        check(mclccd_traverse(h_, V0, V1, nv_, P, mem_));
+        self->dispatch(V0, V1);
+    }
+
+    // Re-runs traverse on the arrays of the last update (no copies).
+    void traverse() const
+    {
+        auto *self = const_cast<BVHTree *>(this);
+        self->push_options();
+        check(mclccd_traverse(h_, nullptr, nullptr, 0, nullptr, mem_));
+        self->dispatch(nullptr, nullptr);
+    }
+
+#ifdef MCLCCD_B200_HAVE_EIGEN
+    // Eigen convenience overloads (BVHTree.hpp:151-186): RowMajor copies, as
+    // the reference makes.
+    template <typename DerivedV, typename DerivedP>
+    void update(const Eigen::MatrixBase<DerivedV> &V0, const Eigen::MatrixBase<DerivedV> &V1,
+                const Eigen::MatrixBase<DerivedP> &P, const Eigen::VectorXi &active = Eigen::VectorXi())
+    {
+        if (V0.rows() != V1.rows()) throw CCDError(MCLCCD_ERR_INVALID, "V0 and V1 row counts differ");
+        RowV v0 = V0.template cast<double>(), v1 = V1.template cast<double>();
+        RowP p = P.template cast<int>();
+        const int *act = active.size() == V0.rows() ? active.data() : nullptr;
+        update(v0.data(), v1.data(), (int)v0.rows(), p.data(), (int)p.rows(), (int)p.cols(), act, MCLCCD_MEM_HOST);
+    }
+    template <typename DerivedV, typename DerivedP>
+    void traverse(const Eigen::MatrixBase<DerivedV> &V0, const Eigen::MatrixBase<DerivedV> &V1,
+                  const Eigen::MatrixBase<DerivedP> &P)
+    {
+        if (V0.rows() != V1.rows()) throw CCDError(MCLCCD_ERR_INVALID, "V0 and V1 row counts differ");
+        RowV v0 = V0.template cast<double>(), v1 = V1.template cast<double>();
+        RowP p = P.template cast<int>();
+        traverse(v0.data(), v1.data(), p.data());
+    }
+#endif
+
+    // ---- results of the last traverse, as arrays ---------------------------
+    long long num_hits() const { long long n = 0; check(mclccd_counts(h_, &n, nullptr, nullptr, nullptr, nullptr)); return n; }
+    long long num_discrete() const { long long n = 0; check(mclccd_counts(h_, nullptr, &n, nullptr, nullptr, nullptr)); return n; }
+    void hits(std::vector<int> &sten, std::vector<unsigned char> &is_vf, std::vector<double> &toi) const
+    {
+        const long long n = num_hits();
+        sten.resize(4 * n); is_vf.resize(n); toi.resize(n);
+        check(mclccd_get_hits(h_, MCLCCD_MEM_HOST, n, sten.data(), is_vf.data(), toi.data()));
+    }
+    void discrete(std::vector<int> &pairs) const
+    {
+        const long long n = num_discrete();
+        pairs.resize(2 * n);
+        check(mclccd_get_discrete(h_, MCLCCD_MEM_HOST, n, pairs.data()));
+    }
+    void candidates(std::vector<int> &sten, std::vector<unsigned char> &is_vf) const
+    {
+        long long nvf = 0, nee = 0;
+        check(mclccd_counts(h_, nullptr, nullptr, &nvf, &nee, nullptr));
+        sten.resize(4 * (nvf + nee)); is_vf.resize(nvf + nee);
+        check(mclccd_get_candidates(h_, MCLCCD_MEM_HOST, nvf + nee, sten.data(), is_vf.data()));
+    }
+    mclccd_tree *handle() const { return h_; }
+
+private:
+#ifdef MCLCCD_B200_HAVE_EIGEN
+    typedef Eigen::Matrix<double, Eigen::Dynamic, DIM, Eigen::RowMajor> RowV;
+    typedef Eigen::Matrix<int, Eigen::Dynamic, Eigen::Dynamic, Eigen::RowMajor> RowP;
+#endif
+    mclccd_tree *h_ = nullptr;
+    int nv_ = 0, np_ = 0, mem_ = MCLCCD_MEM_HOST;
+
+    void check(int rc) const
+    {
+        if (rc != MCLCCD_OK) {
+            const char *m = h_ ? mclccd_last_error(h_) : "";
+            throw CCDError(rc, std::string(mclccd_status_string(rc)) + (m && *m ? std::string(": ") + m : ""));
+        }
+    }
+    void push_options()
+    {
+        unsigned f = 0;
+        if (options.reptri) f |= MCLCCD_OPT_REPTRI;
+        if (options.threaded) f |= MCLCCD_OPT_THREADED;
+        if (options.discrete) f |= MCLCCD_OPT_DISCRETE;
+        if (options.continuous) f |= MCLCCD_OPT_CONTINUOUS;
+        if (options.vf_one_sided) f |= MCLCCD_OPT_VF_ONE_SIDED;
+        if (options.ee_robust) f |= MCLCCD_OPT_EE_ROBUST;
+        check(mclccd_set_options(h_, options.box_eta, options.vf_ccd_eta, options.ee_ccd_eta, f));
+    }
+    void pull_options()
+    {
+        mclccd_get_options(h_, &options.box_eta, &options.vf_ccd_eta, &options.ee_ccd_eta, nullptr);
+    }
+    static Stencil make_stencil(const int *s)
+    {
+        Stencil t;
+        for (int i = 0; i < 4; ++i) t[i] = s[i];
+        return t;
+    }
+    void dispatch(const double *V0, const double *V1)
+    {
+        if (filter_pair || narrow_phase) {
+            std::vector<int> cs;
+            std::vector<unsigned char> cv;
+            candidates(cs, cv);
+            std::vector<int> ks;
+            std::vector<unsigned char> kv;
+            for (size_t i = 0; i < cv.size(); ++i) {
+                if (filter_pair && filter_pair(make_stencil(&cs[4 * i]), cv[i] != 0)) continue;
+                ks.insert(ks.end(), cs.begin() + 4 * i, cs.begin() + 4 * i + 4);
+                kv.push_back(cv[i]);
+            }
+            std::vector<double> toi(kv.size(), -1.0);
+            if (narrow_phase) {
+                for (size_t i = 0; i < kv.size(); ++i) toi[i] = narrow_phase(make_stencil(&ks[4 * i]), kv[i] != 0);
+            } else if (!kv.empty()) {
+                if (!V0 || mem_ != MCLCCD_MEM_HOST)
+                    throw CCDError(MCLCCD_ERR_INVALID, "filter_pair without narrow_phase needs host V0/V1 at traverse");
+                std::vector<int> hit(kv.size());
+                check(mclccd_narrow_phase_bulk(DIM, V0, V1, nv_, ks.data(), kv.data(), (long long)kv.size(),
+                                               options.vf_ccd_eta, options.ee_ccd_eta, toi.data(), hit.data(),
+                                               MCLCCD_MEM_HOST, nullptr));
+            }
+            if (append_pair)
+                for (size_t i = 0; i < kv.size(); ++i)
+                    if (toi[i] >= 0) append_pair(make_stencil(&ks[4 * i]), kv[i] != 0, toi[i]);
+        } else if (append_pair) {
+            std::vector<int> s;
+            std::vector<unsigned char> v;
+            std::vector<double> t;
+            hits(s, v, t);
+            for (size_t i = 0; i < v.size(); ++i) append_pair(make_stencil(&s[4 * i]), v[i] != 0, t[i]);
+        }
+        if (append_discrete && options.discrete) {
+            std::vector<int> d;
+            discrete(d);
+            for (size_t i = 0; i < d.size() / 2; ++i)
+                if (append_discrete(d[2 * i], d[2 * i + 1])) break;
+        }
+    }
+};
+
+} // namespace mcl
