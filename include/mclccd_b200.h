@@ -39,6 +39,7 @@ typedef struct mclccd_tree mclccd_tree;
 #define MCLCCD_ERR_STATE 5       /* traverse before update, or results before traverse */
 #define MCLCCD_ERR_DEVICE 6      /* a kernel gave up a bounded wait or overflowed its stack */
 #define MCLCCD_ERR_UNSUPPORTED 7 /* option not provided by this path (vf_one_sided) */
+#define MCLCCD_ERR_SCRATCH_LIMIT 8 /* mclccd_narrow_phase_bulk_static: arrays exceed its fixed scratch */
 
 /* Where caller arrays live. */
 #define MCLCCD_MEM_HOST 0
@@ -130,6 +131,26 @@ int mclccd_get_leaves(mclccd_tree *tree, double *boxes, unsigned char *flags);
 int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv, const int *sten,
                              const unsigned char *is_vf, long long n, double vf_ccd_eta, double ee_ccd_eta,
                              double *out_toi, int *out_hit, int mem_kind, void *stream);
+
+/* No counterpart in the reference.  The bulk narrow phase above without any
+ * device allocation, for callers that cannot call cudaMalloc: loops on a
+ * fixed device-memory budget (cudaMalloc/cudaFree can stall the device and
+ * fragment the budget), processes where another allocator already holds the
+ * device memory, plugins whose host forbids device allocations.  Same
+ * arguments and results as mclccd_narrow_phase_bulk (bit-identical).  Its
+ * scratch -- the device status word and, for MCLCCD_MEM_HOST, the device
+ * copies of V0, V1, sten, is_vf, out_toi and out_hit, each rounded up to 256
+ * bytes -- lives in one fixed device array of MCLCCD_STATIC_SCRATCH_BYTES
+ * that every GPU loading the library holds until exit; larger host-memory
+ * calls return MCLCCD_ERR_SCRATCH_LIMIT (device-memory calls use only the
+ * status word and have no size limit).  The first call on each device looks
+ * up the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race on it. */
+#define MCLCCD_STATIC_SCRATCH_BYTES (32u << 20)
+int mclccd_narrow_phase_bulk_static(int dim, const double *V0, const double *V1, int nv, const int *sten,
+                                    const unsigned char *is_vf, long long n, double vf_ccd_eta, double ee_ccd_eta,
+                                    double *out_toi, int *out_hit, int mem_kind, void *stream);
 
 /* Per-stage device times (ms) of the last update + traverse when
  * MCLCCD_OPT_PROFILE is set: [update_total, build, refit, traverse_total,

@@ -137,6 +137,7 @@ const char *mclccd_status_string(int s)
     case MCLCCD_ERR_STATE: return "call out of order";
     case MCLCCD_ERR_DEVICE: return "device-side failure (bounded wait or stack)";
     case MCLCCD_ERR_UNSUPPORTED: return "unsupported option";
+    case MCLCCD_ERR_SCRATCH_LIMIT: return "arrays exceed the fixed scratch of mclccd_narrow_phase_bulk_static";
     }
     return "unknown status";
 }
