@@ -147,19 +147,26 @@ __device__ __forceinline__ double pair_distance(const double (&x)[DIM + 1][DIM])
 // computing it).  Returns 1 on hit; toi is the sum of accepted steps.
 // (The iteration-0 skip is taken only when it cannot change a single bit.)
 // iters receives the loop index at exit (0 for an immediate hit).
+//
+// The work is split into setup / head / tail so that other forms (the FP32
+// certified pass) can share the exact FP64 pieces.
 // ---------------------------------------------------------------------------
-template <int DIM, bool VF>
-__device__ __forceinline__ int accd(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM],
-                                    double xsi, double &toi, int &iters)
+
+// Relative motion p_i = (v1_i - v0_i) - mean, start positions x = v0 and --
+// when WANT_LP -- l_p = max first |p| + max second |p| (NarrowPhase.cpp:647-670).
+// step0_noop: x + 0 * p == x bit for bit (every p finite, no x is -0.0, the
+// only value whose bits change: -0.0 + 0.0 == +0.0).
+template <int DIM, bool VF, bool WANT_LP>
+__device__ __forceinline__ void accd_setup(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM],
+                                           double (&p)[DIM + 1][DIM], double (&x)[DIM + 1][DIM], double &l_p,
+                                           bool &step0_noop)
 {
     constexpr int ns = DIM + 1;
-    double p[ns][DIM], x[ns][DIM], pbar[DIM];
+    double pbar[DIM];
 #pragma unroll
     for (int k = 0; k < DIM; ++k) pbar[k] = 0.0;
     const double w = 1.0 / (double)ns;
-    // x + 0 * p == x bit for bit when every p is finite and no x is -0.0
-    // (the only value whose bits change: -0.0 + 0.0 == +0.0).
-    bool step0_noop = true;
+    step0_noop = true;
 #pragma unroll
     for (int i = 0; i < ns; ++i)
 #pragma unroll
@@ -178,25 +185,68 @@ __device__ __forceinline__ int accd(const double (&v0)[DIM + 1][DIM], const doub
             sq = (k == 0) ? p[i][k] * p[i][k] : sq + p[i][k] * p[i][k];
             step0_noop = step0_noop && isfinite(p[i][k]) && !(x[i][k] == 0.0 && signbit(x[i][k]));
         }
-        const double n = sqrt(sq);
-        const bool first = VF ? (i == 0) : (i <= 1);
-        if (first) lf = lf < n ? n : lf;
-        else ls = ls < n ? n : ls;
+        if constexpr (WANT_LP) {
+            const double n = sqrt(sq);
+            const bool first = VF ? (i == 0) : (i <= 1);
+            if (first) lf = lf < n ? n : lf;
+            else ls = ls < n ? n : ls;
+        }
     }
-    const double l_p = lf + ls;
-    iters = -1;
-    if (l_p <= 0) return 0;
+    if constexpr (WANT_LP) l_p = lf + ls;
+}
 
+// Iterations 1..999 of the reference loop, from the state after iteration 0
+// (positions x, accumulated toi, next step t_l, threshold g).
+template <int DIM, bool VF>
+__device__ __forceinline__ int accd_tail(double (&x)[DIM + 1][DIM], const double (&p)[DIM + 1][DIM], double l_p,
+                                         double xsi, double g, double &toi, double t_l, int &iters)
+{
+    constexpr int ns = DIM + 1;
+    const double xx = xsi * xsi;
+    for (int iter = 1; iter < 1000; ++iter) {
+        const bool can_break = toi > 0;
+        if (!can_break && toi + t_l > 1.0) { toi = toi + t_l; iters = iter; return 0; }
+#pragma unroll
+        for (int i = 0; i < ns; ++i)
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) x[i][k] = x[i][k] + t_l * p[i][k];
+        const double d = pair_distance<DIM, VF>(x);
+        const double A = d * d - xx;
+        if (can_break && A / (d + xsi) < g) { iters = iter; return 1; }
+        toi = toi + t_l;
+        if (toi > 1.0) { iters = iter; return 0; }
+        t_l = 0.9 * A / ((d + xsi) * l_p);
+    }
+    iters = 1000;
+    return 1;
+}
+
+// Outcome of ACCD's head (everything before iteration 1).
+enum AccdHead { kHeadMiss = 0, kHeadHit = 1, kHeadContinue = 2 };
+
+// Head: l_p test, first distance, immediate hit, iteration 0, and the miss
+// that iteration 1 would report before its distance is used.  On
+// kHeadContinue, (x, toi, t_l, g) is the state entering iteration 1; d0 is
+// the first distance.  exact_skip tells whether iteration 0 was skipped
+// (then x == v0, toi == 0 and t_l is a function of d0 and l_p alone).
+template <int DIM, bool VF>
+__device__ __forceinline__ int accd_head(double (&x)[DIM + 1][DIM], const double (&p)[DIM + 1][DIM], double l_p,
+                                         bool step0_noop, double xsi, double &d0, double &g, double &toi,
+                                         double &t_l, bool &exact_skip)
+{
+    constexpr int ns = DIM + 1;
+    exact_skip = false;
+    if (l_p <= 0) return kHeadMiss;
     double d = pair_distance<DIM, VF>(x);
+    d0 = d;
     const double xx = xsi * xsi;
     double A = d * d - xx;
-    const double g = (1.0 * A) / (d - xsi);
+    g = (1.0 * A) / (d - xsi);
     toi = 0.0;
-    double t_l = ((1.0 - 1.0) * A) / ((d + xsi) * l_p);
-    if (d <= xsi) { iters = 0; return 1; }
-
-    // iteration 0
-    if (!(t_l == 0.0 && step0_noop)) {
+    t_l = ((1.0 - 1.0) * A) / ((d + xsi) * l_p);
+    if (d <= xsi) return kHeadHit;
+    exact_skip = t_l == 0.0 && step0_noop;
+    if (!exact_skip) {   // iteration 0, literally
 #pragma unroll
         for (int i = 0; i < ns; ++i)
 #pragma unroll
@@ -205,25 +255,25 @@ __device__ __forceinline__ int accd(const double (&v0)[DIM + 1][DIM], const doub
         A = d * d - xx;
     }
     toi = toi + t_l;
-    if (toi > 1.0) { iters = 0; return 0; }
+    if (toi > 1.0) return kHeadMiss;
     t_l = 0.9 * A / ((d + xsi) * l_p);
+    if (!(toi > 0) && toi + t_l > 1.0) return kHeadMiss;   // iteration 1 returns "miss"
+    return kHeadContinue;
+}
 
-    for (int iter = 1; iter < 1000; ++iter) {
-        const bool can_break = toi > 0;
-        if (!can_break && toi + t_l > 1.0) { toi = toi + t_l; iters = iter; return 0; }
-#pragma unroll
-        for (int i = 0; i < ns; ++i)
-#pragma unroll
-            for (int k = 0; k < DIM; ++k) x[i][k] = x[i][k] + t_l * p[i][k];
-        d = pair_distance<DIM, VF>(x);
-        A = d * d - xx;
-        if (can_break && A / (d + xsi) < g) { iters = iter; return 1; }
-        toi = toi + t_l;
-        if (toi > 1.0) { iters = iter; return 0; }
-        t_l = 0.9 * A / ((d + xsi) * l_p);
-    }
-    iters = 1000;
-    return 1;
+template <int DIM, bool VF>
+__device__ __forceinline__ int accd(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM],
+                                    double xsi, double &toi, int &iters)
+{
+    constexpr int ns = DIM + 1;
+    double p[ns][DIM], x[ns][DIM], l_p, d0, g, t_l;
+    bool noop, skip;
+    accd_setup<DIM, VF, true>(v0, v1, p, x, l_p, noop);
+    iters = -1;
+    const int h = accd_head<DIM, VF>(x, p, l_p, noop, xsi, d0, g, toi, t_l, skip);
+    if (h == kHeadHit) { iters = 0; return 1; }
+    if (h == kHeadMiss) { iters = l_p <= 0 ? -1 : 0; return 0; }
+    return accd_tail<DIM, VF>(x, p, l_p, xsi, g, toi, t_l, iters);
 }
 
 // ---------------------------------------------------------------------------

@@ -99,6 +99,26 @@ def test_scenes_against_port(port, scene):
     check_against_port(t, port, V0, V1, F, eta)
 
 
+def test_touching_boxes(port):
+    """Boxes that touch exactly, or miss by one FP64 ulp: the FP32 brackets
+    cannot decide these, so the exact FP64 test must."""
+    rng = np.random.default_rng(5)
+    tris, V = [], []
+    for i in range(400):
+        x0 = 0.3 * (i % 20)
+        y0 = 0.3 * (i // 20)
+        gap = [0.0, 5e-17, -5e-17, 1e-16][i % 4]
+        base = len(V)
+        V += [[x0, y0, 0.0], [x0 + 0.2 + gap, y0, 0.0], [x0, y0 + 0.2 - gap, 0.0]]
+        tris.append([base, base + 1, base + 2])
+    V0 = np.array(V, np.float64)
+    V1 = V0 + rng.normal(0, 1e-9, V0.shape) * (rng.random(V0.shape) < 0.3)
+    F = np.array(tris, np.int32)
+    t = run_gpu(V0, V1, F, 0.05)
+    p = check_against_port(t, port, V0, V1, F, 0.05)
+    assert len(p["leaf_pairs"]) > 500
+
+
 def test_refit_equals_rebuild(port):
     V0, V1, F, eta = scenes.wavy_cloth(97, seed=1)
     V1b = scenes.wavy_redraw(V0, 77)
