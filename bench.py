@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32cert"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tune", default="", help="launch knobs, e.g. walk_packet=0,accd_grid=2368")
     return ap.parse_args()
 
 
@@ -208,6 +209,8 @@ def run_b200(args, rank, world, local):
     tree = BVHTree(3, precision=prec)
     tree.options.box_eta = tree.options.vf_ccd_eta = tree.options.ee_ccd_eta = eta
     tree.options.profile = True
+    if args.tune:
+        tree.set_tuning(**{k: int(v) for k, v in (kv.split("=") for kv in args.tune.split(","))})
     tree.set_stream(stream.cuda_stream)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
 

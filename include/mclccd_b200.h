@@ -157,6 +157,17 @@ int mclccd_narrow_phase_bulk_static(int dim, const double *V0, const double *V1,
  * tree_walk, expand, narrow]; returns how many were written. */
 int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
 
+/* No counterpart in the reference: launch-shape knobs of the device path
+ * (chosen by the autotuner, mclccd_b200/autotune.py).  Keys: grid size (in
+ * blocks) of the stencil-expansion kernel and of the ACCD kernels, and the
+ * tree-walk form (1: warp-cooperative packets, 0: one query per thread). */
+#define MCLCCD_TUNE_EXPAND_GRID 0
+#define MCLCCD_TUNE_ACCD_GRID 1
+#define MCLCCD_TUNE_WALK_PACKET 2
+#define MCLCCD_TUNE_COUNT 3
+int mclccd_set_tuning(mclccd_tree *tree, int key, int value);
+int mclccd_get_tuning(const mclccd_tree *tree, int key, int *value);
+
 /* Kernels launched by this handle since creation (for launch accounting). */
 int mclccd_kernel_launches(const mclccd_tree *tree, long long *n);
 

@@ -25,7 +25,7 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libmclccd_b200.so")
+LIB_PATH = os.environ.get("MCLCCD_B200_LIB") or os.path.join(_HERE, "libmclccd_b200.so")
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_OVERFLOW, ERR_STATE, ERR_DEVICE, ERR_UNSUPPORTED = range(8)
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -70,6 +70,8 @@ def lib():
         "mclccd_narrow_phase_bulk": ([C.c_int, vp, vp, C.c_int, vp, vp, C.c_longlong, C.c_double, C.c_double,
                                       vp, vp, C.c_int, vp], C.c_int),
         "mclccd_stage_ms": ([vp, C.POINTER(C.c_float), C.c_int], C.c_int),
+        "mclccd_set_tuning": ([vp, C.c_int, C.c_int], C.c_int),
+        "mclccd_get_tuning": ([vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mclccd_kernel_launches": ([vp, llp], C.c_int),
         "mclccd_last_error": ([vp], C.c_char_p),
         "mclccd_status_string": ([C.c_int], C.c_char_p),
@@ -177,6 +179,21 @@ class BVHTree:
 
     def set_precision(self, precision: int):
         self._check(self._L.mclccd_set_precision(self._h, precision), self._h)
+
+    TUNE_KEYS = {"expand_grid": 0, "accd_grid": 1, "walk_packet": 2}
+
+    def set_tuning(self, **kv):
+        """Launch-shape knobs (expand_grid, accd_grid, walk_packet)."""
+        for k, v in kv.items():
+            self._check(self._L.mclccd_set_tuning(self._h, self.TUNE_KEYS[k], int(v)), self._h)
+
+    def get_tuning(self) -> dict:
+        out = {}
+        for k, key in self.TUNE_KEYS.items():
+            v = C.c_int()
+            self._check(self._L.mclccd_get_tuning(self._h, key, C.byref(v)), self._h)
+            out[k] = v.value
+        return out
 
     def set_stream(self, stream_handle: int | None):
         self._check(self._L.mclccd_set_stream(self._h, C.c_void_p(stream_handle or 0)), self._h)

@@ -65,6 +65,7 @@ struct mclccd_tree {
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
     cudaEvent_t ev[8] = {};
+    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0};
 };
 
 namespace {
@@ -423,23 +424,24 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
         MC_CUDA(t, ensure(t->hit_isvf, t->cap_hits));
         MC_CUDA(t, ensure(t->disc, sizeof(int2) * t->cap_disc));
         MC_CUDA(t, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
-        launch_traverse(dim, as<Node>(t->nodes), t->leaf_box.p, as<unsigned char>(t->leaf_active), as<int>(t->vals), np,
-                        as<int2>(t->pairs), t->cap_pairs, cnt, st);
+        launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], as<Node>(t->nodes), t->leaf_box.p,
+                        as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
+                        cnt, st);
         if (prof) cudaEventRecord(t->ev[4], st);
         launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
                             as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
-                            cont, discr, cnt, kExpandGrid, st);
+                            cont, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st);
         if (prof) cudaEventRecord(t->ev[5], st);
         t->launches += 2;
         if (cont) {
             launch_accd_pipeline(dim, true, as<int4>(t->vf), &cnt->n_vf, t->cap_vf, dV0, dV1, nv, t->vf_eta,
                                  as<int4>(t->hit_sten), as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf),
-                                 t->cap_hits, cnt, kAccdGrid, st);
+                                 t->cap_hits, cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], st);
             ++t->launches;
             if (dim == 3) {
                 launch_accd_pipeline(dim, false, as<int4>(t->ee), &cnt->n_ee, t->cap_ee, dV0, dV1, nv, t->ee_eta,
                                      as<int4>(t->hit_sten), as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf),
-                                     t->cap_hits, cnt, kAccdGrid, st);
+                                     t->cap_hits, cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], st);
                 ++t->launches;
             }
         }
@@ -660,6 +662,22 @@ int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)
     int k = std::min(n, 7);
     for (int i = 0; i < k; ++i) ms[i] = t->stage[i];
     return k;
+}
+
+int mclccd_set_tuning(mclccd_tree *t, int key, int value)
+{
+    if (!t || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
+    if (key == MCLCCD_TUNE_WALK_PACKET ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))
+        return fail(t, MCLCCD_ERR_INVALID, "tuning value out of range");
+    t->tune[key] = value;
+    return MCLCCD_OK;
+}
+
+int mclccd_get_tuning(const mclccd_tree *t, int key, int *value)
+{
+    if (!t || !value || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
+    *value = t->tune[key];
+    return MCLCCD_OK;
 }
 
 int mclccd_kernel_launches(const mclccd_tree *t, long long *n)

@@ -29,9 +29,16 @@ __device__ __forceinline__ bool gather_stencil(const int *s, const double *__res
     return ok;
 }
 
+// Resident 128-thread blocks per SM the pipeline ACCD kernel is compiled for
+// (register cap = 64K / (128 x this)); the kernel is latency-bound, so more
+// resident warps beat a few spilled registers.
+#ifndef MCLCCD_ACCD_MIN_BLOCKS
+#define MCLCCD_ACCD_MIN_BLOCKS 8
+#endif
+
 // Pipeline form: stencils from the expansion kernel, count read on device.
 template <int DIM, bool VF>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, MCLCCD_ACCD_MIN_BLOCKS)
 k_accd_pipeline(const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
                 const double *__restrict__ V0, const double *__restrict__ V1, int nv, double eta,
                 int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,

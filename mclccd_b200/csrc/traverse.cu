@@ -15,7 +15,17 @@
 
 namespace mclccd {
 
-constexpr int kStackDepth = 64;
+// Traversal stack entries per thread (shared memory) and resident blocks per
+// SM the walk is compiled for.  A Karras tree's depth is at most 30 key bits
+// plus log2 of the largest run of equal keys; overflow is reported
+// (kErrStack), never silent.
+#ifndef MCLCCD_WALK_STACK
+#define MCLCCD_WALK_STACK 64
+#endif
+#ifndef MCLCCD_WALK_MIN_BLOCKS
+#define MCLCCD_WALK_MIN_BLOCKS 1
+#endif
+constexpr int kStackDepth = MCLCCD_WALK_STACK;
 
 // Three-valued leaf test.  Each stored FP32 bound brackets its FP64 value: a
 // min rounded down (L) means the FP64 min lies in [L, next_up(L)], a max
@@ -71,7 +81,7 @@ __device__ __forceinline__ int leaf_test3(const Box2T<DIM> &q, const Box2T<DIM> 
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, MCLCCD_WALK_MIN_BLOCKS)
 k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
            const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
            int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
@@ -137,6 +147,93 @@ k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf
             if (sp == 0) break;
             node = stack[--sp][tid];
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-cooperative ("packet") form of the same walk.  The 32 queries of a warp
+// are consecutive in Morton order, so their boxes are close: the warp walks
+// the tree once, every lane tests each visited node's children against its
+// own box, and the warp descends into a child when any lane needs it.
+// Control flow is warp-uniform (one stack per warp, in shared memory); each
+// lane still applies exactly its own tests, so the pairs found are the same.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(128)
+k_traverse_packet(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
+                  const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
+                  int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
+{
+    constexpr int S = DIM == 3 ? 3 : 2;
+    __shared__ int wstack[4][kStackDepth];
+    const int warp = threadIdx.x >> 5;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (__all_sync(0xffffffffu, q >= n - 1)) return;   // whole warp past the end
+    const bool valid = q < n - 1;
+    const int qq = valid ? q : n - 1;
+    bool qact = false;
+    int qprim = 0;
+    Box2T<DIM> qbox;
+    {
+        const LeafBox<DIM> qb = leaf_box[qq];
+        qact = leaf_active[qq] != 0;
+        qprim = sorted[qq];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
+            qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
+        }
+    }
+    const Box2T<DIM> qin = inner<DIM>(qbox);
+
+    auto leaf = [&](int k, const Box2T<DIM> &kbox) {
+        int r = leaf_test3<DIM>(qbox, qin, kbox);
+        if (r == 2) r = leaf_boxes_intersect<DIM>(leaf_box[qq], leaf_box[k]) ? 1 : 0;
+        if (r == 1) {
+            const int kprim = __ldg(sorted + k);
+            unsigned long long slot = warp_append(&cnt->n_pairs);
+            if (slot < cap) pairs[slot] = make_int2(min(qprim, kprim), max(qprim, kprim));
+        }
+    };
+
+    int sp = 0;      // warp-uniform
+    int node = 0;    // warp-uniform
+    for (int steps = 0;; ++steps) {
+        if (steps >= n) { if ((threadIdx.x & 31) == 0) atomicOr(&cnt->err, kErrStack); break; }
+        float4 ls[S], rs[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) { ls[i] = __ldg(&nodes[node].l[i]); rs[i] = __ldg(&nodes[node].r[i]); }
+        const int4 d = __ldg(&nodes[node].d);
+        const int split = d.x, meta = d.y, last = d.z;
+        Box2T<DIM> lb, rb;
+        unpack_child<DIM>(ls, lb);
+        unpack_child<DIM>(rs, rb);
+        const bool lact = ((meta >> 8) & 0xff) != 0, ract = ((meta >> 16) & 0xff) != 0;
+        bool lok = valid && split > q && (qact || lact);
+        bool rok = valid && last > q && (qact || ract);
+        if (meta & kMetaLeftLeaf) { if (lok) leaf(split, lb); lok = false; }
+        if (meta & kMetaRightLeaf) { if (rok) leaf(split + 1, rb); rok = false; }
+        lok = lok && boxes_may_intersect<DIM>(qbox, lb);
+        rok = rok && boxes_may_intersect<DIM>(qbox, rb);
+        const bool anyl = __any_sync(0xffffffffu, lok), anyr = __any_sync(0xffffffffu, rok);
+        if (anyl) {
+            if (anyr) {
+                if (sp < kStackDepth) {
+                    if ((threadIdx.x & 31) == 0) wstack[warp][sp] = split + 1;
+                    ++sp;
+                } else if ((threadIdx.x & 31) == 0) {
+                    atomicOr(&cnt->err, kErrStack);
+                }
+            }
+            node = split;
+        } else if (anyr) {
+            node = split + 1;
+        } else {
+            if (sp == 0) break;
+            __syncwarp();
+            node = wstack[warp][--sp];
+        }
+        __syncwarp();
     }
 }
 
@@ -248,17 +345,20 @@ k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, cons
     }
 }
 
-void launch_traverse(int dim, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
+void launch_traverse(int dim, int packet, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
                      const int *sorted, int n, int2 *pairs, unsigned long long cap, Counters *cnt, cudaStream_t st)
 {
     if (n < 2) return;
     const int g = (n - 1 + 127) / 128;
-    if (dim == 3)
-        k_traverse<3><<<g, 128, 0, st>>>(nodes, reinterpret_cast<const LeafBox<3> *>(leaf_box), leaf_active, sorted, n,
-                                         pairs, cap, cnt);
-    else
-        k_traverse<2><<<g, 128, 0, st>>>(nodes, reinterpret_cast<const LeafBox<2> *>(leaf_box), leaf_active, sorted, n,
-                                         pairs, cap, cnt);
+    const auto *lb3 = reinterpret_cast<const LeafBox<3> *>(leaf_box);
+    const auto *lb2 = reinterpret_cast<const LeafBox<2> *>(leaf_box);
+    if (packet) {
+        if (dim == 3) k_traverse_packet<3><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, pairs, cap, cnt);
+        else k_traverse_packet<2><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, pairs, cap, cnt);
+    } else {
+        if (dim == 3) k_traverse<3><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, pairs, cap, cnt);
+        else k_traverse<2><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, pairs, cap, cnt);
+    }
 }
 
 void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,
