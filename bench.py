@@ -261,6 +261,7 @@ def run_b200(args, rank, world, local):
         total_max, sten_all = total_s, float(sten)
     value = sten_all / total_max
     c = tree.counts()
+    pstats = tree.precision_stats()
     stage = {k: float(np.median([s[k] for s in stages])) for k in stages[0]}
 
     # roofline of the dominant kernel: algorithmic bytes / its device time
@@ -332,6 +333,7 @@ def run_b200(args, rank, world, local):
                        "tris": n, "stencils_per_step": int(c["vf"] + c["ee"]), "vf": int(c["vf"]),
                        "ee": int(c["ee"]), "hits": int(c["hits"]), "discrete": int(c["discrete"]),
                        "leaf_pairs": int(c["leaf_pairs"]), "first_update_ms": first_ms,
+                       "fp64_stencils": pstats[0], "toi_bound_hits": pstats[1],
                        "precision": args.precision, "parallelism": f"replicas x{world}",
                        "l2": "flushed between timed steps (512 MB write outside the timed events)",
                        "stage_ms_median": stage, "step_ms_all": step_ms},

@@ -132,6 +132,22 @@ int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv
                              const unsigned char *is_vf, long long n, double vf_ccd_eta, double ee_ccd_eta,
                              double *out_toi, int *out_hit, int mem_kind, void *stream);
 
+/* The bulk narrow phase with a precision: MCLCCD_PREC_FP64 (same as above) or
+ * MCLCCD_PREC_FP32_CERTIFIED (identical hit/miss; toi never later than the
+ * FP64 value and within 1e-6 relative of it).  n_fp64 (may be NULL) receives
+ * how many stencils the certified form had to evaluate in full FP64. */
+int mclccd_narrow_phase_bulk_ex(int dim, const double *V0, const double *V1, int nv, const int *sten,
+                                const unsigned char *is_vf, long long n, double vf_ccd_eta, double ee_ccd_eta,
+                                double *out_toi, int *out_hit, int mem_kind, void *stream, int precision,
+                                long long *n_fp64);
+
+/* Stencils of the last traverse that the FP32-certified form handed to its
+ * FP64 pass (ACCD undecided by the FP32 brackets), and hits it reported with
+ * the certified lower bound on toi (within 1e-6 relative) instead of the
+ * bit-identical FP64 value (both 0 in MCLCCD_PREC_FP64 mode).  Either pointer
+ * may be NULL. */
+int mclccd_precision_stats(const mclccd_tree *tree, long long *n_fp64, long long *n_bound_toi);
+
 /* No counterpart in the reference.  The bulk narrow phase above without any
  * device allocation, for callers that cannot call cudaMalloc: loops on a
  * fixed device-memory budget (cudaMalloc/cudaFree can stall the device and

@@ -70,6 +70,9 @@ def lib():
         "mclccd_narrow_phase_bulk": ([C.c_int, vp, vp, C.c_int, vp, vp, C.c_longlong, C.c_double, C.c_double,
                                       vp, vp, C.c_int, vp], C.c_int),
         "mclccd_stage_ms": ([vp, C.POINTER(C.c_float), C.c_int], C.c_int),
+        "mclccd_narrow_phase_bulk_ex": ([C.c_int, vp, vp, C.c_int, vp, vp, C.c_longlong, C.c_double, C.c_double,
+                                         vp, vp, C.c_int, vp, C.c_int, llp], C.c_int),
+        "mclccd_precision_stats": ([vp, llp, llp], C.c_int),
         "mclccd_set_tuning": ([vp, C.c_int, C.c_int], C.c_int),
         "mclccd_get_tuning": ([vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mclccd_kernel_launches": ([vp, llp], C.c_int),
@@ -290,6 +293,16 @@ class BVHTree:
         self._check(self._L.mclccd_get_leaves(self._h, b.ctypes.data, f.ctypes.data), self._h)
         return b, f
 
+    def fp64_fallbacks(self) -> int:
+        """Stencils the FP32-certified form evaluated in full FP64 (last traverse)."""
+        return self.precision_stats()[0]
+
+    def precision_stats(self):
+        """(stencils the FP32-certified form handed to FP64, hits reported with the toi bound)."""
+        n, m = C.c_longlong(), C.c_longlong()
+        self._check(self._L.mclccd_precision_stats(self._h, C.byref(n), C.byref(m)), self._h)
+        return n.value, m.value
+
     def stage_ms(self):
         a = (C.c_float * 7)()
         self._L.mclccd_stage_ms(self._h, a, 7)
@@ -301,29 +314,34 @@ class BVHTree:
         return n.value
 
 
-def narrow_phase_bulk(V0, V1, sten, is_vf, vf_eta, ee_eta=None, stream: int | None = None):
+def narrow_phase_bulk(V0, V1, sten, is_vf, vf_eta, ee_eta=None, stream: int | None = None,
+                      precision: int = PREC_FP64, return_fallbacks: bool = False):
     """NarrowPhaseACCD::query_ccd_vf/ee over a stencil array on the GPU.
-    Returns (toi, hit); toi is -1 where hit == 0."""
+    Returns (toi, hit); toi is -1 where hit == 0.  With
+    precision=PREC_FP32_CERTIFIED and return_fallbacks, also the number of
+    stencils that needed full FP64."""
     L = lib()
     ee_eta = vf_eta if ee_eta is None else ee_eta
+    nfb = C.c_longlong()
     if _is_torch_cuda(V0):
         import torch
         n = sten.shape[0]
         dim = V0.shape[1]
         toi = torch.empty(n, dtype=torch.float64, device=V0.device)
         hit = torch.empty(n, dtype=torch.int32, device=V0.device)
-        rc = L.mclccd_narrow_phase_bulk(dim, V0.data_ptr(), V1.data_ptr(), V0.shape[0], sten.contiguous().data_ptr(),
-                                        is_vf.contiguous().data_ptr(), n, vf_eta, ee_eta, toi.data_ptr(),
-                                        hit.data_ptr(), MEM_DEVICE, C.c_void_p(stream or 0))
+        rc = L.mclccd_narrow_phase_bulk_ex(dim, V0.data_ptr(), V1.data_ptr(), V0.shape[0],
+                                           sten.contiguous().data_ptr(), is_vf.contiguous().data_ptr(), n, vf_eta,
+                                           ee_eta, toi.data_ptr(), hit.data_ptr(), MEM_DEVICE,
+                                           C.c_void_p(stream or 0), precision, C.byref(nfb))
     else:
         V0 = np.ascontiguousarray(V0, np.float64); V1 = np.ascontiguousarray(V1, np.float64)
         s = np.ascontiguousarray(sten, np.int32).reshape(-1, 4)
         v = np.ascontiguousarray(is_vf, np.uint8).reshape(-1)
         n = len(s)
         toi = np.empty(n, np.float64); hit = np.empty(n, np.int32)
-        rc = L.mclccd_narrow_phase_bulk(V0.shape[1], V0.ctypes.data, V1.ctypes.data, V0.shape[0], s.ctypes.data,
-                                        v.ctypes.data, n, vf_eta, ee_eta, toi.ctypes.data, hit.ctypes.data,
-                                        MEM_HOST, C.c_void_p(stream or 0))
+        rc = L.mclccd_narrow_phase_bulk_ex(V0.shape[1], V0.ctypes.data, V1.ctypes.data, V0.shape[0], s.ctypes.data,
+                                           v.ctypes.data, n, vf_eta, ee_eta, toi.ctypes.data, hit.ctypes.data,
+                                           MEM_HOST, C.c_void_p(stream or 0), precision, C.byref(nfb))
     if rc != OK:
         raise CCDError(rc, L.mclccd_status_string(rc).decode())
-    return toi, hit
+    return (toi, hit, nfb.value) if return_fallbacks else (toi, hit)

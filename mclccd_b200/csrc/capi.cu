@@ -49,18 +49,19 @@ struct mclccd_tree {
     const double *upd_V0 = nullptr, *upd_V1 = nullptr;
     long long launches = 0;
     float stage[7] = {0, 0, 0, 0, 0, 0, 0};
-    unsigned long long n_pairs = 0, n_vf = 0, n_ee = 0, n_hits = 0, n_disc = 0;
+    unsigned long long n_pairs = 0, n_vf = 0, n_ee = 0, n_hits = 0, n_disc = 0, n_fp64 = 0, n_bound_toi = 0;
     unsigned long long cap_pairs = 0, cap_vf = 0, cap_ee = 0, cap_hits = 0, cap_disc = 0;
 
     DevBuf V0d, V1d, Pd, Pstage, actd, pflags, pflags_tmp, vowner, ekeys, eowner;
     DevBuf cent, bounds, keys, vals, keys_alt, vals_alt, sort_scratch;
     DevBuf nodes, leaf_parent, visits, leaf_box, leaf_active;
-    DevBuf pairs, vf, ee, hit_sten, hit_toi, hit_isvf, disc, counters, diff;
+    DevBuf pairs, vf, ee, hit_sten, hit_toi, hit_isvf, disc, counters, diff, fp64_queue;
     std::vector<DevBuf *> all()
     {
         return {&V0d, &V1d, &Pd, &Pstage, &actd, &pflags, &pflags_tmp, &vowner, &ekeys, &eowner, &cent, &bounds,
                 &keys, &vals, &keys_alt, &vals_alt, &sort_scratch, &nodes, &leaf_parent, &visits, &leaf_box,
-                &leaf_active, &pairs, &vf, &ee, &hit_sten, &hit_toi, &hit_isvf, &disc, &counters, &diff};
+                &leaf_active, &pairs, &vf, &ee, &hit_sten, &hit_toi, &hit_isvf, &disc, &counters, &diff,
+                &fp64_queue};
     }
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
@@ -423,6 +424,8 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
         MC_CUDA(t, ensure(t->hit_toi, sizeof(double) * t->cap_hits));
         MC_CUDA(t, ensure(t->hit_isvf, t->cap_hits));
         MC_CUDA(t, ensure(t->disc, sizeof(int2) * t->cap_disc));
+        const bool certified = t->precision == MCLCCD_PREC_FP32_CERTIFIED;
+        if (certified && cont) MC_CUDA(t, ensure(t->fp64_queue, sizeof(unsigned) * std::max(t->cap_vf, t->cap_ee)));
         MC_CUDA(t, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
         launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], as<Node>(t->nodes), t->leaf_box.p,
                         as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
@@ -434,16 +437,22 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
         if (prof) cudaEventRecord(t->ev[5], st);
         t->launches += 2;
         if (cont) {
-            launch_accd_pipeline(dim, true, as<int4>(t->vf), &cnt->n_vf, t->cap_vf, dV0, dV1, nv, t->vf_eta,
-                                 as<int4>(t->hit_sten), as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf),
-                                 t->cap_hits, cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], st);
-            ++t->launches;
-            if (dim == 3) {
-                launch_accd_pipeline(dim, false, as<int4>(t->ee), &cnt->n_ee, t->cap_ee, dV0, dV1, nv, t->ee_eta,
-                                     as<int4>(t->hit_sten), as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf),
-                                     t->cap_hits, cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], st);
-                ++t->launches;
-            }
+            // FP32-certified: an FP32 pass and an FP64 pass over its queue per list.
+            auto accd = [&](bool vf, DevBuf &list, unsigned long long *n_ptr, unsigned long long cap, double eta) {
+                if (certified) {
+                    launch_accd_certified(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
+                                          as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits,
+                                          as<unsigned>(t->fp64_queue), cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], st);
+                    t->launches += 2;
+                } else {
+                    launch_accd_pipeline(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
+                                         as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
+                                         t->tune[MCLCCD_TUNE_ACCD_GRID], st);
+                    ++t->launches;
+                }
+            };
+            accd(true, t->vf, &cnt->n_vf, t->cap_vf, t->vf_eta);
+            if (dim == 3) accd(false, t->ee, &cnt->n_ee, t->cap_ee, t->ee_eta);
         }
         if (prof) cudaEventRecord(t->ev[6], st);
         if (int rc = check_launch(t, "traverse kernels")) return rc;
@@ -478,6 +487,8 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
     t->n_ee = c.n_ee;
     t->n_hits = c.n_hits;
     t->n_disc = c.n_discrete;
+    t->n_fp64 = c.n_fp64[0] + c.n_fp64[1];
+    t->n_bound_toi = c.n_bound_toi;
     // kErrAccdIters only notes that some stencil ran ACCD's full 1000
     // iterations (the reference then reports a hit too); it is not a failure.
     const unsigned fatal = c.err & ~kErrAccdIters;
@@ -598,6 +609,16 @@ int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv
                              const unsigned char *is_vf, long long n, double vf_eta, double ee_eta, double *out_toi,
                              int *out_hit, int mem_kind, void *stream)
 {
+    return mclccd_narrow_phase_bulk_ex(dim, V0, V1, nv, sten, is_vf, n, vf_eta, ee_eta, out_toi, out_hit, mem_kind,
+                                       stream, MCLCCD_PREC_FP64, nullptr);
+}
+
+int mclccd_narrow_phase_bulk_ex(int dim, const double *V0, const double *V1, int nv, const int *sten,
+                                const unsigned char *is_vf, long long n, double vf_eta, double ee_eta, double *out_toi,
+                                int *out_hit, int mem_kind, void *stream, int precision, long long *n_fp64)
+{
+    if (n_fp64) *n_fp64 = 0;
+    if (precision != MCLCCD_PREC_FP64 && precision != MCLCCD_PREC_FP32_CERTIFIED) return MCLCCD_ERR_INVALID;
     if ((dim != 2 && dim != 3) || n < 0 || nv < 0) return MCLCCD_ERR_INVALID;
     if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return MCLCCD_ERR_INVALID;
     if (!(vf_eta >= 0) || !(ee_eta >= 0)) return MCLCCD_ERR_INVALID;
@@ -607,8 +628,10 @@ int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv
     const size_t vbytes = sizeof(double) * (size_t)nv * dim;
     // Scratch: the device error word, plus device copies of host arrays.
     char *scratch = nullptr;
-    size_t off_cnt = 0, off_v0 = 256, off_v1 = 0, off_s = 0, off_f = 0, off_t = 0, off_h = 0, total = 256;
+    // FP32-certified: plus the queue of stencils for the FP64 pass.
+    size_t off_cnt = 0, off_q = 256, off_v0 = 256, off_v1 = 0, off_s = 0, off_f = 0, off_t = 0, off_h = 0, total = 256;
     auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    if (precision == MCLCCD_PREC_FP32_CERTIFIED) total = off_v0 = off_q + align(sizeof(long long) * (size_t)n);
     if (mem_kind == MCLCCD_MEM_HOST) {
         off_v1 = off_v0 + align(vbytes);
         off_s = off_v1 + align(vbytes);
@@ -640,7 +663,11 @@ int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv
         if (e == cudaSuccess) e = cudaMemcpyAsync((void *)df, is_vf, (size_t)n, cudaMemcpyHostToDevice, st);
     }
     if (e == cudaSuccess) {
-        launch_accd_bulk(dim, ds, df, n, dV0, dV1, nv, vf_eta, ee_eta, dt, dh, cnt, st);
+        if (precision == MCLCCD_PREC_FP32_CERTIFIED)
+            launch_accd_certified_bulk(dim, ds, df, n, dV0, dV1, nv, vf_eta, ee_eta, dt, dh,
+                                       reinterpret_cast<long long *>(scratch + off_q), cnt, st);
+        else
+            launch_accd_bulk(dim, ds, df, n, dV0, dV1, nv, vf_eta, ee_eta, dt, dh, cnt, st);
         e = cudaGetLastError();
     }
     Counters h{};
@@ -653,7 +680,16 @@ int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv
     cudaFreeAsync(scratch, st);
     if (e != cudaSuccess) rc = MCLCCD_ERR_CUDA;
     else if (h.err & kErrBadIndex) rc = MCLCCD_ERR_INVALID;
+    if (n_fp64) *n_fp64 = (long long)(h.n_fp64[0] + h.n_fp64[1]);
     return rc;
+}
+
+int mclccd_precision_stats(const mclccd_tree *t, long long *n_fp64, long long *n_bound_toi)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (n_fp64) *n_fp64 = (long long)t->n_fp64;
+    if (n_bound_toi) *n_bound_toi = (long long)t->n_bound_toi;
+    return MCLCCD_OK;
 }
 
 int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)

@@ -32,7 +32,8 @@ struct Counters {
     unsigned long long n_ee;
     unsigned long long n_hits;
     unsigned long long n_discrete;
-    unsigned long long n_certified;   // FP32 form: stencils decided in FP64
+    unsigned long long n_fp64[2];     // FP32 form: stencils queued for FP64 (VF / EE lists)
+    unsigned long long n_bound_toi;   // FP32 form: hits reported with the certified toi bound
     unsigned int err;
     unsigned int pad;
 };

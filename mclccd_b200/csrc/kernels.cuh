@@ -36,6 +36,14 @@ void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap
 void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
                           unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st);
+// certified.cu
+void launch_accd_certified(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr,
+                           unsigned long long cap, const double *V0, const double *V1, int nv, double eta,
+                           int4 *hit_sten, double *hit_toi, unsigned char *hit_isvf, unsigned long long hit_cap,
+                           unsigned *queue, Counters *cnt, int grid, cudaStream_t st);
+void launch_accd_certified_bulk(int dim, const int *sten, const unsigned char *is_vf, long long n, const double *V0,
+                                const double *V1, int nv, double vf_eta, double ee_eta, double *out_toi, int *out_hit,
+                                long long *queue, Counters *cnt, cudaStream_t st);
 void launch_accd_bulk(int dim, const int *sten, const unsigned char *is_vf, long long n, const double *V0,
                       const double *V1, int nv, double vf_eta, double ee_eta, double *out_toi, int *out_hit,
                       Counters *cnt, cudaStream_t st);

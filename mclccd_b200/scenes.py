@@ -176,3 +176,47 @@ def batch_scenes(n3d: int = 384, n2d: int = 128, seed: int = 0, max_side: int = 
         ring = int(rng.integers(32, max_ring + 1))
         scenes.append(("annulus", annulus_2d(ring, seed=seed * 104729 + s)))
     return scenes
+
+
+def stress_stencils(n: int = 100_000, seed: int = 0, eta: float = 1e-3):
+    """Constructed hard stencils for the precision form: half near-parallel
+    edge-edge pairs (angle <= 1e-7 rad), half near-coplanar vertex-face pairs
+    (the point within the separation of the triangle's plane), separations
+    log-uniform in [1e-8, 1e-2], each pair closing along its normal by a
+    random fraction of up to twice the gap (some hit, some miss).
+    Returns V0, V1 (4n x 3), sten (n x 4), is_vf (n), eta."""
+    rng = np.random.default_rng(seed)
+    sep = np.exp(rng.uniform(np.log(1e-8), np.log(1e-2), n))
+    base = rng.uniform(0.0, 1.0, (n, 3))
+    u = rng.normal(size=(n, 3)); u /= np.linalg.norm(u, axis=1, keepdims=True)
+    w = rng.normal(size=(n, 3)); w -= (w * u).sum(1, keepdims=True) * u; w /= np.linalg.norm(w, axis=1, keepdims=True)
+    nrm = np.cross(u, w)
+    L = rng.uniform(1e-3, 5e-2, n)[:, None]
+    V0 = np.empty((4 * n, 3)); V1 = np.empty((4 * n, 3))
+    is_vf = (np.arange(n) % 2 == 0).astype(np.uint8)
+    close = (eta + sep)[:, None] * rng.uniform(0.0, 2.0, (n, 1))
+    # vertex-face: triangle (a, a+L u, a+L w); point above its interior (or
+    # just outside) at height eta + sep, moving down by `close`.
+    a = base
+    off = rng.uniform(-0.1, 0.6, (n, 2))
+    pt = a + L * (off[:, :1] * u + off[:, 1:] * w) + (eta + sep)[:, None] * nrm
+    # edge-edge: edge (a, a + L u) and a copy tilted by <= 1e-7 rad, offset by
+    # eta + sep along the normal, moving toward it by `close`.
+    ang = rng.uniform(-1e-7, 1e-7, n)[:, None]
+    dirb = u * np.cos(ang) + nrm * np.sin(ang)
+    shift = rng.uniform(-0.5, 0.5, n)[:, None] * L
+    q0 = a + shift * u + (eta + sep)[:, None] * nrm
+    q1 = q0 + L * dirb
+    vf = is_vf == 1
+    V0[0::4] = np.where(vf[:, None], pt, a)
+    V0[1::4] = np.where(vf[:, None], a, a + L * u)
+    V0[2::4] = np.where(vf[:, None], a + L * u, q0)
+    V0[3::4] = np.where(vf[:, None], a + L * w, q1)
+    V1[:] = V0
+    mv = close * nrm
+    V1[0::4] -= np.where(vf[:, None], mv, 0.0)
+    V1[2::4] -= np.where(vf[:, None], 0.0, mv)
+    V1[3::4] -= np.where(vf[:, None], 0.0, mv)
+    V1 += rng.normal(0.0, 1e-12, V1.shape)
+    sten = (np.arange(4 * n, dtype=np.int32).reshape(n, 4))
+    return V0, V1, sten, is_vf, eta
