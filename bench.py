@@ -21,6 +21,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -46,6 +47,7 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32cert"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the certified/adjoint/batch form measurements")
     ap.add_argument("--tune", default="", help="launch knobs, e.g. walk_packet=0,accd_grid=2368")
     return ap.parse_args()
 
@@ -70,12 +72,26 @@ class Clocks:
         self.p = None
 
     def start(self):
+        """Starts the sampler and returns once it is producing samples, so the
+        region that follows is covered from its first millisecond."""
+        self.n0 = 0
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+            # line-buffered, so a sample reaches the file when it is taken
+            pre = ["stdbuf", "-oL"] if shutil.which("stdbuf") else []
+            self.p = subprocess.Popen(pre + ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                             "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.p.poll() is None:
+            with open(self.f.name) as fh:
+                n = sum(1 for _ in fh)
+            if n >= 1:
+                self.n0 = n
+                return
+            time.sleep(0.02)
 
     def stop(self):
         if self.p is None:
@@ -88,9 +104,9 @@ class Clocks:
         self.f.flush()
         rows = []
         with open(self.f.name) as fh:
-            for line in fh:
+            for k, line in enumerate(fh):
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
+                if k >= self.n0 - 1 and len(parts) >= 9:   # from the last sample before the region on
                     rows.append(parts)
         os.unlink(self.f.name)
         if not rows:
@@ -315,6 +331,10 @@ def run_b200(args, rank, world, local):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e_total * 1e3 / args.steps}
 
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(V0, V1a, V1b, F, eta, c["vf"] + c["ee"])
@@ -340,10 +360,94 @@ def run_b200(args, rank, world, local):
             "gpu_launches": int(launches), "roofline": roof, "clocks": clk}
     if e2e is not None:
         line["e2e"] = e2e
+    if forms is not None:
+        line["forms"] = forms
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
+
+
+def measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev):
+    """The other forms, on one GPU: the FP32-certified narrow phase on the
+    same workload as the headline (other precision than the headline's), and
+    the toi adjoint on the 256 x 256 folded cloth (forward = update +
+    traverse + ACCD, backward = the VJP over all hits)."""
+    import torch
+    from mclccd_b200 import PREC_FP32_CERTIFIED, PREC_FP64, BVHTree, scenes
+    out = {}
+
+    def timed(fn, k, w):
+        for _ in range(w):
+            fn()
+        ms = []
+        for _ in range(k):
+            flush.zero_()
+            a, b = ev(), ev()
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return float(np.median(ms)), ms
+
+    # precision form: the other precision on the headline workload
+    other = PREC_FP64 if tree.precision == PREC_FP32_CERTIFIED else PREC_FP32_CERTIFIED
+    t2 = BVHTree(3, precision=other)
+    t2.options.box_eta = t2.options.vf_ccd_eta = t2.options.ee_ccd_eta = eta
+    t2.options.profile = True
+    t2.set_stream(stream.cuda_stream)
+    t2.update(dV0, V1s[1], dF)
+    t2.traverse()
+    it = [0]
+    stg = []
+
+    def step():
+        t2.update(dV0, V1s[it[0] % 2], dF)
+        t2.traverse()
+        it[0] += 1
+        stg.append(t2.stage_ms())
+
+    ms, _ = timed(step, max(3, min(args.steps, 6)), 2)
+    narrow2 = float(np.median([s["narrow"] for s in stg[2:]]))
+    fp64_narrow, cert_narrow = (stage["narrow"], narrow2) if other == PREC_FP32_CERTIFIED else (narrow2, stage["narrow"])
+    ps = t2.precision_stats() if other == PREC_FP32_CERTIFIED else tree.precision_stats()
+    c2 = t2.counts()
+    out["fp32_certified"] = {
+        "workload": "headline workload, other precision than the headline line",
+        "ms_per_step_" + ("fp32cert" if other == PREC_FP32_CERTIFIED else "fp64"): ms,
+        "narrow_ms_fp64": fp64_narrow, "narrow_ms_fp32cert": cert_narrow,
+        "narrow_speedup_fp32cert_vs_fp64": fp64_narrow / cert_narrow,
+        "fp64_pass_stencils": ps[0], "toi_bound_hits": ps[1], "hits": int(c2["hits"]),
+        "stencils": int(c2["vf"] + c2["ee"])}
+    del t2
+
+    # differentiation form: 256 x 256 folded cloth, thickness 1e-3
+    V0, V1, F, eta4 = scenes.folded_cloth(256)
+    a0, a1, aF = (torch.from_numpy(x).to(dev) for x in (V0, V1, F))
+    t3 = BVHTree(3, precision=PREC_FP64)
+    t3.options.box_eta = t3.options.vf_ccd_eta = t3.options.ee_ccd_eta = eta4
+    t3.set_stream(stream.cuda_stream)
+
+    def fwd():
+        t3.update(a0, a1, aF)
+        t3.traverse()
+
+    fwd()
+    nh = t3.counts()["hits"]
+    g = torch.randn(nh, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+    res = {}
+
+    def bwd():
+        res["v"] = t3.vjp_toi(g)
+
+    f_ms, _ = timed(fwd, 5, 2)
+    b_ms, _ = timed(bwd, 5, 2)
+    out["adjoint"] = {"workload": f"folded cloth 256x256 ({len(F)} tris), thickness 1e-3, FP64",
+                      "forward_ms": f_ms, "backward_ms": b_ms, "backward_to_forward": b_ms / f_ms,
+                      "hits": int(nh), "hits_with_gradient": int(res["v"][2])}
+    del t3
+    return out
 
 
 def main():

@@ -168,6 +168,40 @@ int mclccd_narrow_phase_bulk_static(int dim, const double *V0, const double *V1,
                                     const unsigned char *is_vf, long long n, double vf_ccd_eta, double ee_ccd_eta,
                                     double *out_toi, int *out_hit, int mem_kind, void *stream);
 
+/* No counterpart in the reference: the adjoint of the time of impact.
+ * For each hit (stencil, is_vf, toi as ACCD reported it) the contact time t*
+ * is the first root t >= toi of dist(x(t)) = eta with x(t) = V0 + t (V1 - V0)
+ * (true closest points, FP64), refined from toi; its gradient follows from
+ * implicit differentiation of that contact condition, recomputing the
+ * closest-feature pair at t*.  Outputs (each may be NULL):
+ *   dV0, dV1   nv x dim, overwritten with sum_h g_toi[h] d(t*_h)/dV0 (resp. V1)
+ *              (the vector-Jacobian product a torch.autograd.Function
+ *              backward computes; needs g_toi);
+ *   t_star     n contact times;  status  n MCLCCD_VJP_* codes;
+ *   jac_rows   n x 2 (dim+1) dim: d(t*)/dV0 of the stencil's dim+1 vertices,
+ *              then d(t*)/dV1, slot-major;
+ *   n_ok       how many hits had a gradient (status MCLCCD_VJP_OK).
+ * A hit whose status is not OK contributes zero.  All arrays on the same side
+ * (mem_kind). */
+#define MCLCCD_VJP_OK 0
+#define MCLCCD_VJP_TOI_ZERO 1   /* toi == 0 (within eta at t = 0): constant */
+#define MCLCCD_VJP_NO_CONTACT 2 /* dist stays above eta on [toi, 1] */
+#define MCLCCD_VJP_GRAZING 3    /* d/dt dist ~ 0 at t*: not differentiable */
+#define MCLCCD_VJP_NO_CONVERGE 4
+#define MCLCCD_VJP_BAD_TOI 5    /* toi outside [0, 1], or no root at all */
+#define MCLCCD_VJP_BAD_INDEX 6  /* stencil vertex outside [0, nv) */
+int mclccd_vjp_toi(int dim, const double *V0, const double *V1, int nv, const int *sten, const unsigned char *is_vf,
+                   const double *toi, const double *g_toi, long long n, double vf_ccd_eta, double ee_ccd_eta,
+                   double *dV0, double *dV1, double *t_star, int *status, double *jac_rows, long long *n_ok,
+                   int mem_kind, void *stream);
+
+/* The same for the hits of the handle's last traverse, in mclccd_get_hits
+ * order, with the V0/V1 that traverse used (device copies or the caller's
+ * device arrays, which must still be valid) and the handle's etas.  g_toi has
+ * one entry per hit; dV0/dV1 are nv x dim; all on the mem_kind side. */
+int mclccd_tree_vjp_toi(mclccd_tree *tree, const double *g_toi, double *dV0, double *dV1, long long *n_ok,
+                        int mem_kind);
+
 /* Per-stage device times (ms) of the last update + traverse when
  * MCLCCD_OPT_PROFILE is set: [update_total, build, refit, traverse_total,
  * tree_walk, expand, narrow]; returns how many were written. */

@@ -73,6 +73,9 @@ def lib():
         "mclccd_narrow_phase_bulk_ex": ([C.c_int, vp, vp, C.c_int, vp, vp, C.c_longlong, C.c_double, C.c_double,
                                          vp, vp, C.c_int, vp, C.c_int, llp], C.c_int),
         "mclccd_precision_stats": ([vp, llp, llp], C.c_int),
+        "mclccd_vjp_toi": ([C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, C.c_longlong, C.c_double, C.c_double, vp, vp,
+                            vp, vp, vp, llp, C.c_int, vp], C.c_int),
+        "mclccd_tree_vjp_toi": ([vp, vp, vp, vp, llp, C.c_int], C.c_int),
         "mclccd_set_tuning": ([vp, C.c_int, C.c_int], C.c_int),
         "mclccd_get_tuning": ([vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mclccd_kernel_launches": ([vp, llp], C.c_int),
@@ -140,6 +143,7 @@ class BVHTree:
     def __init__(self, dim: int = 3, precision: int = PREC_FP64):
         self._L = lib()
         self.dim = dim
+        self._nv = 0
         h = C.c_void_p()
         self._check(self._L.mclccd_create(dim, C.byref(h)), None)
         self._h = h
@@ -150,6 +154,7 @@ class BVHTree:
         self.narrow_phase = None
         self._keep = []
         self._last = None
+        self.precision = PREC_FP64
         if precision != PREC_FP64:
             self.set_precision(precision)
 
@@ -182,6 +187,7 @@ class BVHTree:
 
     def set_precision(self, precision: int):
         self._check(self._L.mclccd_set_precision(self._h, precision), self._h)
+        self.precision = precision
 
     TUNE_KEYS = {"expand_grid": 0, "accd_grid": 1, "walk_packet": 2}
 
@@ -219,6 +225,7 @@ class BVHTree:
         self._pull_options()
         self._check(rc, self._h)
         self._keep = [a0, a1, ap, aa]
+        self._nv = nv
 
     def traverse(self, V0=None, V1=None, P=None):
         """BVHTree::traverse (BVHTree.cpp:129-159), then the hooks."""
@@ -228,6 +235,8 @@ class BVHTree:
         kind = k0 if k0 is not None else MEM_HOST
         self._push_options()
         self._check(self._L.mclccd_traverse(self._h, pv0, pv1, nv, pp, kind), self._h)
+        if V0 is not None:
+            self._nv = nv
         self._dispatch(V0, V1)
 
     def _dispatch(self, V0, V1):
@@ -303,6 +312,29 @@ class BVHTree:
         self._check(self._L.mclccd_precision_stats(self._h, C.byref(n), C.byref(m)), self._h)
         return n.value, m.value
 
+    def vjp_toi(self, g_toi):
+        """Adjoint of the last traverse's hits: (dL/dV0, dL/dV1, n_ok) for the
+        upstream gradient g_toi (one entry per hit, in hits() order).  numpy
+        in, numpy out; a CUDA tensor in gives CUDA tensors out."""
+        n_ok = C.c_longlong()
+        cnt = self.counts()
+        if _is_torch_cuda(g_toi):
+            import torch
+            g = g_toi.to(torch.float64).contiguous()
+            nv, dim = self._nv, self.dim
+            dV0 = torch.empty((nv, dim), dtype=torch.float64, device=g.device)
+            dV1 = torch.empty_like(dV0)
+            self._check(self._L.mclccd_tree_vjp_toi(self._h, g.data_ptr(), dV0.data_ptr(), dV1.data_ptr(),
+                                                    C.byref(n_ok), MEM_DEVICE), self._h)
+            return dV0, dV1, n_ok.value
+        g = np.ascontiguousarray(g_toi, np.float64).reshape(-1)
+        if len(g) != cnt["hits"]:
+            raise ValueError(f"g_toi has {len(g)} entries, the traverse had {cnt['hits']} hits")
+        dV0 = np.zeros((self._nv, self.dim)); dV1 = np.zeros((self._nv, self.dim))
+        self._check(self._L.mclccd_tree_vjp_toi(self._h, g.ctypes.data, dV0.ctypes.data, dV1.ctypes.data,
+                                                C.byref(n_ok), MEM_HOST), self._h)
+        return dV0, dV1, n_ok.value
+
     def stage_ms(self):
         a = (C.c_float * 7)()
         self._L.mclccd_stage_ms(self._h, a, 7)
@@ -345,3 +377,40 @@ def narrow_phase_bulk(V0, V1, sten, is_vf, vf_eta, ee_eta=None, stream: int | No
     if rc != OK:
         raise CCDError(rc, L.mclccd_status_string(rc).decode())
     return (toi, hit, nfb.value) if return_fallbacks else (toi, hit)
+
+
+def vjp_toi(V0, V1, sten, is_vf, toi, g_toi=None, vf_eta=1e-6, ee_eta=None, want_rows: bool = False,
+            stream: int | None = None):
+    """Adjoint of the time of impact over a hit array (mclccd_vjp_toi).
+
+    Returns a dict: t_star, status (MCLCCD_VJP_*), n_ok, and with g_toi the
+    vector-Jacobian products dV0, dV1 (nv x dim); with want_rows the per-hit
+    Jacobian rows (n x 2 (dim+1) dim: d(t*)/dV0 slots, then d(t*)/dV1 slots).
+    numpy arrays in host memory (the device path is the C call with
+    MCLCCD_MEM_DEVICE)."""
+    L = lib()
+    ee_eta = vf_eta if ee_eta is None else ee_eta
+    V0 = np.ascontiguousarray(V0, np.float64); V1 = np.ascontiguousarray(V1, np.float64)
+    nv, dim = V0.shape
+    s = np.ascontiguousarray(sten, np.int32).reshape(-1, 4)
+    v = np.ascontiguousarray(is_vf, np.uint8).reshape(-1)
+    t = np.ascontiguousarray(toi, np.float64).reshape(-1)
+    n = len(s)
+    g = None if g_toi is None else np.ascontiguousarray(g_toi, np.float64).reshape(-1)
+    dV0 = np.zeros((nv, dim)) if g is not None else None
+    dV1 = np.zeros((nv, dim)) if g is not None else None
+    ts = np.empty(n); st = np.empty(n, np.int32)
+    rows = np.empty((n, 2 * (dim + 1) * dim)) if want_rows else None
+    n_ok = C.c_longlong()
+    ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+    rc = L.mclccd_vjp_toi(dim, V0.ctypes.data, V1.ctypes.data, nv, s.ctypes.data, v.ctypes.data, t.ctypes.data,
+                          ptr(g), n, vf_eta, ee_eta, ptr(dV0), ptr(dV1), ts.ctypes.data, st.ctypes.data, ptr(rows),
+                          C.byref(n_ok), MEM_HOST, C.c_void_p(stream or 0))
+    if rc != OK:
+        raise CCDError(rc, L.mclccd_status_string(rc).decode())
+    out = {"t_star": ts, "status": st, "n_ok": n_ok.value}
+    if g is not None:
+        out["dV0"], out["dV1"] = dV0, dV1
+    if want_rows:
+        out["rows"] = rows
+    return out

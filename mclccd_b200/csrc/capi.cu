@@ -47,6 +47,8 @@ struct mclccd_tree {
     bool built = false, traversed = false;
     int np = 0, pdim = 0, nv = 0, flags_np = 0;
     const double *upd_V0 = nullptr, *upd_V1 = nullptr;
+    const double *tr_V0 = nullptr, *tr_V1 = nullptr;   // device V0/V1 of the last traverse
+    int tr_nv = 0;
     long long launches = 0;
     float stage[7] = {0, 0, 0, 0, 0, 0, 0};
     unsigned long long n_pairs = 0, n_vf = 0, n_ee = 0, n_hits = 0, n_disc = 0, n_fp64 = 0, n_bound_toi = 0;
@@ -406,6 +408,9 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
         }
     }
     const int np = t->np;
+    t->tr_V0 = dV0;
+    t->tr_V1 = dV1;
+    t->tr_nv = nv;
     const bool cont = (t->flags & MCLCCD_OPT_CONTINUOUS) != 0;
     const bool discr = (t->flags & MCLCCD_OPT_DISCRETE) != 0;
     if (t->cap_pairs == 0) {
@@ -681,6 +686,115 @@ int mclccd_narrow_phase_bulk_ex(int dim, const double *V0, const double *V1, int
     if (e != cudaSuccess) rc = MCLCCD_ERR_CUDA;
     else if (h.err & kErrBadIndex) rc = MCLCCD_ERR_INVALID;
     if (n_fp64) *n_fp64 = (long long)(h.n_fp64[0] + h.n_fp64[1]);
+    return rc;
+}
+
+int mclccd_vjp_toi(int dim, const double *V0, const double *V1, int nv, const int *sten, const unsigned char *is_vf,
+                   const double *toi, const double *g_toi, long long n, double vf_eta, double ee_eta, double *dV0,
+                   double *dV1, double *t_star, int *status, double *jac_rows, long long *n_ok, int mem_kind,
+                   void *stream)
+{
+    if (n_ok) *n_ok = 0;
+    if ((dim != 2 && dim != 3) || n < 0 || nv < 0) return MCLCCD_ERR_INVALID;
+    if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return MCLCCD_ERR_INVALID;
+    if (!(vf_eta >= 0) || !(ee_eta >= 0)) return MCLCCD_ERR_INVALID;
+    if ((dV0 != nullptr) != (dV1 != nullptr)) return MCLCCD_ERR_INVALID;
+    if (dV0 && !g_toi) return MCLCCD_ERR_INVALID;
+    if (n > 0 && (!V0 || !V1 || !sten || !is_vf || !toi || nv == 0)) return MCLCCD_ERR_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t vbytes = sizeof(double) * (size_t)nv * dim, un = (size_t)n;
+    const size_t rbytes = sizeof(double) * un * 2 * (dim + 1) * dim;
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    // Scratch: the counter, plus device copies of host arrays.
+    size_t off[11] = {0};
+    const size_t sizes[11] = {sizeof(unsigned long long), vbytes, vbytes, sizeof(int) * 4 * un, un,
+                              sizeof(double) * un, g_toi ? sizeof(double) * un : 0, dV0 ? vbytes : 0,
+                              dV0 ? vbytes : 0, t_star ? sizeof(double) * un : 0, status ? sizeof(int) * un : 0};
+    const bool host = mem_kind == MCLCCD_MEM_HOST;
+    size_t total = 0;
+    for (int i = 0; i < 11; ++i) {
+        off[i] = total;
+        if (i == 0 || host) total += align(sizes[i]);
+    }
+    size_t off_rows = total;
+    if (host && jac_rows) total += align(rbytes);
+    char *scratch = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&scratch), total, st);
+    if (e != cudaSuccess) { cudaGetLastError(); return e == cudaErrorMemoryAllocation ? MCLCCD_ERR_NOMEM : MCLCCD_ERR_CUDA; }
+    auto dev = [&](int i, const void *p) -> void * { return host ? (p ? scratch + off[i] : nullptr) : const_cast<void *>(p); };
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(scratch);
+    const double *dv0 = (const double *)dev(1, V0), *dv1 = (const double *)dev(2, V1);
+    const int *ds = (const int *)dev(3, sten);
+    const unsigned char *df = (const unsigned char *)dev(4, is_vf);
+    const double *dt = (const double *)dev(5, toi), *dg = (const double *)dev(6, g_toi);
+    double *gV0 = (double *)dev(7, dV0), *gV1 = (double *)dev(8, dV1), *dts = (double *)dev(9, t_star);
+    int *dst = (int *)dev(10, status);
+    double *drows = host ? (jac_rows ? reinterpret_cast<double *>(scratch + off_rows) : nullptr) : jac_rows;
+    e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st);
+    if (host) {
+        const void *src[7] = {nullptr, V0, V1, sten, is_vf, toi, g_toi};
+        for (int i = 1; i < 7 && e == cudaSuccess; ++i)
+            if (src[i] && sizes[i]) e = cudaMemcpyAsync(scratch + off[i], src[i], sizes[i], cudaMemcpyHostToDevice, st);
+    }
+    if (e == cudaSuccess && gV0) e = cudaMemsetAsync(gV0, 0, vbytes, st);
+    if (e == cudaSuccess && gV1) e = cudaMemsetAsync(gV1, 0, vbytes, st);
+    if (e == cudaSuccess) {
+        launch_vjp_toi(dim, ds, df, dt, dg, n, dv0, dv1, nv, vf_eta, ee_eta, gV0, gV1, dts, dst, drows, cnt, st);
+        e = cudaGetLastError();
+    }
+    unsigned long long h_ok = 0;
+    if (host && e == cudaSuccess) {
+        if (dV0) e = cudaMemcpyAsync(dV0, gV0, vbytes, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && dV1) e = cudaMemcpyAsync(dV1, gV1, vbytes, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && t_star && n) e = cudaMemcpyAsync(t_star, dts, sizeof(double) * un, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && status && n) e = cudaMemcpyAsync(status, dst, sizeof(int) * un, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && jac_rows && n) e = cudaMemcpyAsync(jac_rows, drows, rbytes, cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_ok, cnt, sizeof(h_ok), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFreeAsync(scratch, st);
+    if (e != cudaSuccess) return MCLCCD_ERR_CUDA;
+    if (n_ok) *n_ok = (long long)h_ok;
+    return MCLCCD_OK;
+}
+
+int mclccd_tree_vjp_toi(mclccd_tree *t, const double *g_toi, double *dV0, double *dV1, long long *n_ok, int mem_kind)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!t->traversed) return fail(t, MCLCCD_ERR_STATE, "no traverse results");
+    if (t->n_hits > t->cap_hits) return fail(t, MCLCCD_ERR_STATE, "hit buffer overflowed");
+    if (t->n_hits > 0 && !t->tr_V0) return fail(t, MCLCCD_ERR_STATE, "no traverse geometry");
+    DeviceGuard g(t->device);
+    const int dim = t->dim;
+    const long long n = (long long)t->n_hits;
+    // Device-side stencils of the hits; V0/V1 are the traverse's device arrays.
+    const int *sten = as<int>(t->hit_sten);
+    const unsigned char *is_vf = as<unsigned char>(t->hit_isvf);
+    const double *toi = as<double>(t->hit_toi);
+    if (mem_kind == MCLCCD_MEM_DEVICE)
+        return mclccd_vjp_toi(dim, t->tr_V0, t->tr_V1, t->tr_nv, sten, is_vf, toi, g_toi, n, t->vf_eta, t->ee_eta, dV0,
+                              dV1, nullptr, nullptr, nullptr, n_ok, MCLCCD_MEM_DEVICE, t->stream);
+    if (mem_kind != MCLCCD_MEM_HOST) return MCLCCD_ERR_INVALID;
+    // Host g / dV: stage through device scratch.
+    const size_t vbytes = sizeof(double) * (size_t)t->tr_nv * dim;
+    double *dg = nullptr, *d0 = nullptr, *d1 = nullptr;
+    cudaStream_t st = t->stream;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&dg), sizeof(double) * (size_t)std::max<long long>(n, 1), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void **>(&d0), std::max<size_t>(vbytes, 8), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void **>(&d1), std::max<size_t>(vbytes, 8), st);
+    if (e == cudaSuccess && g_toi && n) e = cudaMemcpyAsync(dg, g_toi, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, st);
+    int rc = e == cudaSuccess ? MCLCCD_OK : MCLCCD_ERR_CUDA;
+    if (rc == MCLCCD_OK)
+        rc = mclccd_vjp_toi(dim, t->tr_V0, t->tr_V1, t->tr_nv, sten, is_vf, toi, g_toi ? dg : nullptr, n, t->vf_eta,
+                            t->ee_eta, dV0 ? d0 : nullptr, dV1 ? d1 : nullptr, nullptr, nullptr, nullptr, n_ok,
+                            MCLCCD_MEM_DEVICE, st);
+    if (rc == MCLCCD_OK && dV0) rc = cudaMemcpyAsync(dV0, d0, vbytes, cudaMemcpyDeviceToHost, st) ? MCLCCD_ERR_CUDA : rc;
+    if (rc == MCLCCD_OK && dV1) rc = cudaMemcpyAsync(dV1, d1, vbytes, cudaMemcpyDeviceToHost, st) ? MCLCCD_ERR_CUDA : rc;
+    if (rc == MCLCCD_OK) rc = cudaStreamSynchronize(st) ? MCLCCD_ERR_CUDA : rc;
+    if (dg) cudaFreeAsync(dg, st);
+    if (d0) cudaFreeAsync(d0, st);
+    if (d1) cudaFreeAsync(d1, st);
+    if (rc != MCLCCD_OK) fail(t, rc, "vjp_toi failed");
     return rc;
 }
 

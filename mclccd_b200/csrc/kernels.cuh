@@ -44,6 +44,11 @@ void launch_accd_certified(int dim, bool vf, const int4 *sten, const unsigned lo
 void launch_accd_certified_bulk(int dim, const int *sten, const unsigned char *is_vf, long long n, const double *V0,
                                 const double *V1, int nv, double vf_eta, double ee_eta, double *out_toi, int *out_hit,
                                 long long *queue, Counters *cnt, cudaStream_t st);
+// adjoint.cu
+void launch_vjp_toi(int dim, const int *sten, const unsigned char *is_vf, const double *toi, const double *g,
+                    long long n, const double *V0, const double *V1, int nv, double vf_eta, double ee_eta,
+                    double *dV0, double *dV1, double *t_star, int *status, double *rows, unsigned long long *n_ok,
+                    cudaStream_t st);
 void launch_accd_bulk(int dim, const int *sten, const unsigned char *is_vf, long long n, const double *V0,
                       const double *V1, int nv, double vf_eta, double ee_eta, double *out_toi, int *out_hit,
                       Counters *cnt, cudaStream_t st);

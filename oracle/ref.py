@@ -161,6 +161,12 @@ class Port:
         L.port_discrete.argtypes = [C.c_int, _dp, _ip, _ip, C.c_longlong, _ip]
         L.port_additive_ccd.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_int, _dp, _ip]
         L.port_additive_ccd.restype = C.c_int
+        L.adj_ref_row.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double, _dp, _dp]
+        L.adj_ref_row.restype = C.c_int
+        L.adj_ref_batch.argtypes = [C.c_int, _dp, _dp, _ip, _ucp, _dp, C.c_longlong, C.c_double, C.c_double, _dp,
+                                    _ip, _dp]
+        L.adj_ref_fd.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_double, _dp]
+        L.adj_ref_fd.restype = C.c_int
         self.L = L
 
     def leaf_boxes(self, V0, V1, F, eta, active=None, flags=None):
@@ -247,3 +253,27 @@ class Port:
         else:
             out["discrete"] = np.zeros((0, 2), np.int32)
         return out
+
+    # --- adjoint of the time of impact (oracle/adjoint_ref.c) ---
+    def vjp_rows(self, V0, V1, sten, is_vf, toi, vf_eta, ee_eta=None):
+        """Per hit: (t_star, status, rows) with rows = d(t*)/d(V0 slots, V1 slots)."""
+        dim = V0.shape[1]
+        ee_eta = vf_eta if ee_eta is None else ee_eta
+        V0 = np.ascontiguousarray(V0, np.float64); V1 = np.ascontiguousarray(V1, np.float64)
+        sten = np.ascontiguousarray(sten, np.int32).reshape(-1, 4)
+        is_vf = np.ascontiguousarray(is_vf, np.uint8); toi = np.ascontiguousarray(toi, np.float64)
+        n = len(sten)
+        ts = np.zeros(n); st = np.zeros(n, np.int32); rows = np.zeros((n, 2 * (dim + 1) * dim))
+        self.L.adj_ref_batch(dim, _p(V0, C.c_double), _p(V1, C.c_double), _p(sten, C.c_int), _p(is_vf, C.c_ubyte),
+                             _p(toi, C.c_double), n, vf_eta, ee_eta, _p(ts, C.c_double), _p(st, C.c_int),
+                             _p(rows, C.c_double))
+        return ts, st, rows
+
+    def vjp_fd(self, v0, v1, is_vf, eta, toi, h=1e-7):
+        """Central differences of t* over one stencil's coordinates (v0, v1: (dim+1) x dim)."""
+        v0 = np.ascontiguousarray(v0, np.float64); v1 = np.ascontiguousarray(v1, np.float64)
+        dim = v0.shape[1]
+        out = np.zeros(2 * (dim + 1) * dim)
+        st = self.L.adj_ref_fd(dim, int(is_vf), _p(v0, C.c_double), _p(v1, C.c_double), eta, toi, h,
+                               _p(out, C.c_double))
+        return st, out
