@@ -17,9 +17,9 @@
 //
 // Closest points are the true ones (Ericson, Real-Time Collision Detection,
 // 2005, 5.1.5 point-triangle and 5.1.9 segment-segment), evaluated in FP64.
-// The root is found by safeguarded Newton from toi: conservative advancement
-// t += f / l (l = Lipschitz bound of the distance) where Newton is not safe,
-// Newton inside a bracket once a point past the root is seen.
+// The root is found from toi by conservative advancement along the current
+// separating direction (no root is ever passed; a step beyond t = 1 proves
+// there is none), which converges to the first root quadratically.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -142,26 +142,6 @@ __device__ void eval(const Stencil<DIM, VF> &S, double t, double &d, double (&w)
     for (int k = 0; k < DIM; ++k) { n[k] = sep[k] * inv; ft += n[k] * vel[k]; }
 }
 
-// Support gap at t = 1 along the unit direction n (from the second primitive
-// towards the first): min over the first primitive's vertices of n . x minus
-// the max over the second's.  Vertices move linearly, so this gap is concave
-// in t; with n the separation direction at t it equals dist(t) there, hence
-// dist >= min(dist(t), gap at 1) on all of [t, 1].
-template <int DIM, bool VF>
-__device__ __forceinline__ double end_gap(const Stencil<DIM, VF> &S, const double (&n)[DIM])
-{
-    constexpr int ns = DIM + 1, na = Stencil<DIM, VF>::na;
-    double ga = INFINITY, gb = -INFINITY;
-#pragma unroll
-    for (int i = 0; i < ns; ++i) {
-        double p = 0.0;
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) p += n[k] * (S.x0[i][k] + S.D[i][k]);
-        if (i < na) ga = fmin(ga, p); else gb = fmax(gb, p);
-    }
-    return ga - gb;
-}
-
 // Contact root and Jacobian row for one stencil: row[0..ns*DIM) = dt*/dV0,
 // row[ns*DIM..2 ns*DIM) = dt*/dV1 (slot-major).  Returns the status.
 template <int DIM, bool VF>
@@ -210,52 +190,35 @@ __device__ int toi_gradient(const double (&v0)[DIM + 1][DIM], const double (&v1)
         f = d - eta;
         if (!(f > 0.0)) return kBadToi;
     }
-    // Conservative advancement: t += f / l never passes a root (|f'| <= l),
-    // and a step past t = 1 proves there is none in [t, 1].
-    const double tol = 1e-4 * eta;
-    const double gap_min = eta * (1.0 + 1e-12) + 1e-300;
-    int k = 0;
-    for (; f > tol && k < 4096; ++k) {
-        if (end_gap<DIM, VF>(S, n) > gap_min) return kNoContact;   // separating plane holds to t = 1
-        const double tn = t + f / l;
-        if (tn > 1.0) return kNoContact;
-        if (!(tn > t)) break;
-        t = tn;
-        eval<DIM, VF>(S, t, d, w, n, ft);
-        f = d - eta;
-    }
-    if (f > tol && k >= 4096) return kNoConverge;
-    double lo = t, hi = f > 0.0 ? 2.0 : t;   // hi > 1: no point past the root seen yet
-    // Newton from within 1e-4 eta of the root, safeguarded by a bracket once a
-    // point at or past it is seen; while no bracket and not approaching, the
-    // rigorous advancement step.
+    // Advancement along the separating direction n at t: every vertex moves
+    // linearly, so the support gap along n, min_a n.x_a(tau) - max_b n.x_b(tau),
+    // is bounded below by each pair's linear n.(x_a - x_b)(tau) and never
+    // exceeds the distance.  The largest tau keeping every pair at >= eta is
+    // therefore a step that passes no root; it is at least the Lipschitz step
+    // f / l and, near a contact, the Newton step, so the iterates rise to the
+    // first root quadratically.  A step beyond t = 1 proves there is none.
     bool converged = false;
-    for (int it = 0; it < 64; ++it) {
-        if (f == 0.0) { converged = true; break; }
-        double tn;
-        if (hi <= 1.0) {
-            tn = ft != 0.0 ? t - f / ft : 0.5 * (lo + hi);
-            if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
-        } else if (ft < -1e-12 * l) {
-            tn = t - f / ft;
-            if (tn > 1.0) {
-                double dn, wn[ns], nn[DIM], ftn;
-                eval<DIM, VF>(S, 1.0, dn, wn, nn, ftn);
-                if (dn - eta > 0.0) return kNoContact;
-                hi = 1.0;
-                if (!(tn < hi)) tn = 0.5 * (lo + hi);
+    for (int it = 0; it < 512; ++it) {
+        if (!(f > 0.0)) { converged = true; break; }
+        double tau = INFINITY;
+#pragma unroll
+        for (int a = 0; a < na; ++a)
+#pragma unroll
+            for (int b = na; b < ns; ++b) {
+                double c = 0.0, v = 0.0;
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) {
+                    c += n[k] * ((S.x0[a][k] + t * S.D[a][k]) - (S.x0[b][k] + t * S.D[b][k]));
+                    v += n[k] * (S.D[a][k] - S.D[b][k]);
+                }
+                if (v < 0.0) tau = fmin(tau, (c - eta) / -v);
             }
-        } else {
-            tn = t + f / l;
-            if (tn > 1.0) return kNoContact;
-        }
-        const double step = fabs(tn - t);
-        t = tn;
+        const double step = fmax(tau, f / l);   // both are root-free; rounding can only shrink tau
+        if (t + step > 1.0) return kNoContact;
+        if (!(step > 4e-16 * fmax(1.0, t))) { converged = true; break; }
+        t = t + step;
         eval<DIM, VF>(S, t, d, w, n, ft);
         f = d - eta;
-        if (f > 0.0) lo = t; else hi = t;
-        const double scale = 4e-16 * fmax(1.0, t);
-        if (step <= scale || hi - lo <= scale) { converged = true; break; }
     }
     tstar = t;
     if (!converged) return kNoConverge;

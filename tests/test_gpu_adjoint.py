@@ -112,8 +112,9 @@ def test_tree_vjp_device_tensors():
     h0, h1, nh = t.vjp_toi(g)
     d0, d1, nd = t.vjp_toi(torch.tensor(g, device="cuda"))
     assert nh == nd
-    assert np.allclose(d0.cpu().numpy(), h0, rtol=1e-12, atol=1e-15)
-    assert np.allclose(d1.cpu().numpy(), h1, rtol=1e-12, atol=1e-15)
+    # same terms, summed by atomics in another order
+    assert np.allclose(d0.cpu().numpy(), h0, rtol=1e-12, atol=1e-12 * np.abs(h0).max())
+    assert np.allclose(d1.cpu().numpy(), h1, rtol=1e-12, atol=1e-12 * np.abs(h1).max())
 
 
 def test_adjoint_status_cases():
