@@ -202,6 +202,45 @@ int mclccd_vjp_toi(int dim, const double *V0, const double *V1, int nv, const in
 int mclccd_tree_vjp_toi(mclccd_tree *tree, const double *g_toi, double *dV0, double *dV1, long long *n_ok,
                         int mem_kind);
 
+/* No counterpart in the reference: batched CCD of many independent scenes.
+ * Each scene is what one BVHTree<double, dim> would process (dim 2: P is an
+ * edge list, dim 3: triangles), with box_eta = vf_ccd_eta = ee_ccd_eta =
+ * eta[s] and the default options.  One mclccd_batch_run builds a segmented
+ * LBVH over all scenes and runs one persistent traversal + narrow-phase kernel
+ * with a global work queue, as a CUDA graph (captured on the first run after
+ * the scenes, precision or tuning change, replayed afterwards).  Results are
+ * per-scene reductions rather than hit lists:
+ *   n_hits, n_discrete, n_stencils  hits, discrete pairs and candidate
+ *                                   stencils (VF + EE) of the scene;
+ *   min_toi, min_sten, min_is_vf    earliest toi and its stencil (scene-local
+ *                                   vertex ids; ties go to VF before EE, then
+ *                                   the smallest ids), -1 when no hit;
+ *   done_ms                         when the scene's last work finished,
+ *                                   from the start of the run (device clock);
+ *   batch_ms                        device time of the whole run.
+ * V0/V1/P are the scenes' arrays concatenated in scene order (each scene's
+ * own dim per row); P holds scene-local vertex ids. */
+typedef struct mclccd_batch mclccd_batch;
+#define MCLCCD_BATCH_TUNE_BLOCK 0   /* threads per block of the persistent kernel: 128 or 256 */
+#define MCLCCD_BATCH_TUNE_STACK 1   /* traversal stack entries per thread: 32 or 64 */
+#define MCLCCD_BATCH_TUNE_CHUNK 2   /* queries per lane taken from the work queue at a time: 1..64 */
+#define MCLCCD_BATCH_TUNE_LEAF 3    /* subtrees of up to this many leaves are scanned, not descended: 1..16 */
+#define MCLCCD_BATCH_TUNE_COUNT 4
+int mclccd_batch_create(mclccd_batch **out);
+int mclccd_batch_destroy(mclccd_batch *batch);
+int mclccd_batch_set_scenes(mclccd_batch *batch, int n_scenes, const int *scene_dim, const int *scene_nv,
+                            const int *scene_np, const double *V0, const double *V1, const int *P, const double *eta,
+                            int mem_kind);
+int mclccd_batch_set_positions(mclccd_batch *batch, const double *V0, const double *V1, int mem_kind);
+int mclccd_batch_set_precision(mclccd_batch *batch, int precision);
+int mclccd_batch_set_tuning(mclccd_batch *batch, int key, int value);
+int mclccd_batch_get_tuning(const mclccd_batch *batch, int key, int *value);
+int mclccd_batch_run(mclccd_batch *batch, void *stream);
+int mclccd_batch_results(mclccd_batch *batch, long long *n_hits, double *min_toi, int *min_sten,
+                         unsigned char *min_is_vf, long long *n_discrete, long long *n_stencils, double *done_ms,
+                         double *batch_ms);
+const char *mclccd_batch_last_error(const mclccd_batch *batch);
+
 /* Per-stage device times (ms) of the last update + traverse when
  * MCLCCD_OPT_PROFILE is set: [update_total, build, refit, traverse_total,
  * tree_walk, expand, narrow]; returns how many were written. */

@@ -9,42 +9,9 @@
 // visited once), so the tree shape is free to be the GPU-friendly one.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "lbvh.cuh"
 
 namespace mclccd {
-
-// ---------------------------------------------------------------------------
-// Leaf box of primitive `prim` (BVHTree.cpp:95-119): hull of its vertices at
-// t0 and at t1, padded by eta.  Returns false if a vertex index is invalid.
-// ---------------------------------------------------------------------------
-template <int DIM>
-__device__ __forceinline__ bool compute_leaf_box(const double *__restrict__ V0, const double *__restrict__ V1,
-                                                 const int *__restrict__ P, int pdim, int nv, int prim, double eta,
-                                                 const int *__restrict__ active, LeafBox<DIM> &b, bool &act)
-{
-    bool ok = true;
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) { b.lo0[k] = b.lo1[k] = 1.7976931348623157e308; b.hi0[k] = b.hi1[k] = -1.7976931348623157e308; }
-    act = active == nullptr;
-    for (int j = 0; j < pdim; ++j) {
-        int v = __ldg(P + (size_t)prim * pdim + j);
-        if (v < 0 || v >= nv) { ok = false; continue; }
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) {
-            double a = __ldg(V0 + (size_t)v * DIM + k), c = __ldg(V1 + (size_t)v * DIM + k);
-            if (a < b.lo0[k]) b.lo0[k] = a;
-            if (b.hi0[k] < a) b.hi0[k] = a;
-            if (c < b.lo1[k]) b.lo1[k] = c;
-            if (b.hi1[k] < c) b.hi1[k] = c;
-        }
-        if (active != nullptr && __ldg(active + v)) act = true;
-    }
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        b.lo0[k] -= eta; b.lo1[k] -= eta;
-        b.hi0[k] += eta; b.hi1[k] += eta;
-    }
-    return ok;
-}
 
 // Scene bounds of box centres, as ordered uints: [min(DIM), max(DIM)].
 __global__ void k_init_bounds(unsigned *bounds, int dim)
@@ -87,24 +54,6 @@ __global__ void k_centroids(const double *__restrict__ V0, const double *__restr
             atomicMax(bounds + DIM + k, float_to_ordered(hi[k]));
         }
     }
-}
-
-__device__ __forceinline__ unsigned expand_bits3(unsigned v)   // 10 bits -> every 3rd bit
-{
-    v = (v * 0x00010001u) & 0xFF0000FFu;
-    v = (v * 0x00000101u) & 0x0F00F00Fu;
-    v = (v * 0x00000011u) & 0xC30C30C3u;
-    v = (v * 0x00000005u) & 0x49249249u;
-    return v;
-}
-__device__ __forceinline__ unsigned expand_bits2(unsigned v)   // 15 bits -> every 2nd bit
-{
-    v &= 0x7fffu;
-    v = (v | (v << 8)) & 0x00FF00FFu;
-    v = (v | (v << 4)) & 0x0F0F0F0Fu;
-    v = (v | (v << 2)) & 0x33333333u;
-    v = (v | (v << 1)) & 0x55555555u;
-    return v;
 }
 
 template <int DIM>
@@ -184,46 +133,6 @@ __global__ void k_karras(const unsigned *__restrict__ keys, int n, Node *__restr
 // climbs: the second thread to reach an internal node merges both child slots
 // and moves up (first arrival stops).  `visits` must be zero on entry.
 // ---------------------------------------------------------------------------
-template <int DIM>
-__device__ __forceinline__ void write_child(Node *nodes, int parent, bool right, const Box2T<DIM> &b, bool act)
-{
-    Node *nd = nodes + parent;
-    pack_child<DIM>(right ? nd->r : nd->l, b);
-    reinterpret_cast<unsigned char *>(&nd->d.y)[right ? 2 : 1] = act ? 1 : 0;
-}
-
-template <int DIM>
-__device__ __forceinline__ void merge_children(const Node *nd, Box2T<DIM> &out, bool &act)
-{
-    constexpr int S = DIM == 3 ? 3 : 2;
-    float4 ls[S], rs[S];
-#pragma unroll
-    for (int i = 0; i < S; ++i) { ls[i] = __ldcg(&nd->l[i]); rs[i] = __ldcg(&nd->r[i]); }
-    const int meta = __ldcg(&nd->d.y);
-    act = ((meta >> 8) & 0xff) || ((meta >> 16) & 0xff);
-    Box2T<DIM> a, b;
-    unpack_child<DIM>(ls, a);
-    unpack_child<DIM>(rs, b);
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        out.t0lo[k] = fminf(a.t0lo[k], b.t0lo[k]); out.t0hi[k] = fmaxf(a.t0hi[k], b.t0hi[k]);
-        out.t1lo[k] = fminf(a.t1lo[k], b.t1lo[k]); out.t1hi[k] = fmaxf(a.t1hi[k], b.t1hi[k]);
-    }
-}
-
-// FP32 boxes that contain the FP64 ones (round min down, max up).
-template <int DIM>
-__device__ __forceinline__ Box2T<DIM> outward(const LeafBox<DIM> &b)
-{
-    Box2T<DIM> o;
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        o.t0lo[k] = __double2float_rd(b.lo0[k]); o.t0hi[k] = __double2float_ru(b.hi0[k]);
-        o.t1lo[k] = __double2float_rd(b.lo1[k]); o.t1hi[k] = __double2float_ru(b.hi1[k]);
-    }
-    return o;
-}
-
 template <int DIM>
 __global__ void k_refit(const double *__restrict__ V0, const double *__restrict__ V1, const int *__restrict__ P,
                         int np, int pdim, int nv, double eta, const int *__restrict__ active,

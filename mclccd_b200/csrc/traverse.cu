@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "geom.cuh"
 #include "kernels.cuh"
+#include "lbvh.cuh"
 
 namespace mclccd {
 
@@ -26,59 +27,6 @@ namespace mclccd {
 #define MCLCCD_WALK_MIN_BLOCKS 1
 #endif
 constexpr int kStackDepth = MCLCCD_WALK_STACK;
-
-// Three-valued leaf test.  Each stored FP32 bound brackets its FP64 value: a
-// min rounded down (L) means the FP64 min lies in [L, next_up(L)], a max
-// rounded up (H) means the FP64 max lies in [next_down(H), H].  The
-// reference's predicate (BVHTree.cpp:411-423) is evaluated on those intervals:
-// 1 = true for every FP64 value in the brackets, 0 = false for every one,
-// 2 = cannot tell (then the FP64 boxes decide).  No FP64 data is touched for
-// the clear cases, and the answer is never different from the FP64 test.
-// Upper end of a min's bracket and lower end of a max's bracket:
-// x + |x| 2^-22 (+ 2^-125 for tiny x) with directed rounding is at least one
-// ulp away from x, so [x, up(x)] holds the FP64 min and [dn(x), x] the FP64 max.
-__device__ __forceinline__ float up1(float x) { return __fadd_ru(__fmaf_ru(fabsf(x), 0x1p-22f, x), 0x1p-125f); }
-__device__ __forceinline__ float dn1(float x) { return __fsub_rd(__fmaf_rd(-fabsf(x), 0x1p-22f, x), 0x1p-125f); }
-
-template <int DIM>
-__device__ __forceinline__ Box2T<DIM> inner(const Box2T<DIM> &b)
-{
-    Box2T<DIM> o;
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        o.t0lo[k] = up1(b.t0lo[k]); o.t1lo[k] = up1(b.t1lo[k]);
-        o.t0hi[k] = dn1(b.t0hi[k]); o.t1hi[k] = dn1(b.t1hi[k]);
-    }
-    return o;
-}
-
-// q, c: outward boxes; qi: inner(q).
-template <int DIM>
-__device__ __forceinline__ int leaf_test3(const Box2T<DIM> &q, const Box2T<DIM> &qi, const Box2T<DIM> &c)
-{
-    int res = 1;
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        const float c0lo_u = up1(c.t0lo[k]), c1lo_u = up1(c.t1lo[k]);
-        const float c0hi_d = dn1(c.t0hi[k]), c1hi_d = dn1(c.t1hi[k]);
-        // overlap: min(lo0,lo1) <= max(hi0,hi1) both ways
-        const float qmin_dn = fminf(q.t0lo[k], q.t1lo[k]), qmin_up = fminf(qi.t0lo[k], qi.t1lo[k]);
-        const float qmax_up = fmaxf(q.t0hi[k], q.t1hi[k]), qmax_dn = fmaxf(qi.t0hi[k], qi.t1hi[k]);
-        const float cmin_dn = fminf(c.t0lo[k], c.t1lo[k]), cmin_up = fminf(c0lo_u, c1lo_u);
-        const float cmax_up = fmaxf(c.t0hi[k], c.t1hi[k]), cmax_dn = fmaxf(c0hi_d, c1hi_d);
-        if (qmin_dn > cmax_up || cmin_dn > qmax_up) return 0;
-        if (!(qmin_up <= cmax_dn && cmin_up <= qmax_dn)) res = 2;
-        // separation on this axis at both times, on the same side:
-        // (q.lo0 > c.hi0 && q.lo1 > c.hi1) || (q.hi0 < c.lo0 && q.hi1 < c.lo1)
-        const bool a_true = q.t0lo[k] > c.t0hi[k] && q.t1lo[k] > c.t1hi[k];
-        const bool a_false = qi.t0lo[k] <= c0hi_d || qi.t1lo[k] <= c1hi_d;
-        const bool b_true = q.t0hi[k] < c.t0lo[k] && q.t1hi[k] < c.t1lo[k];
-        const bool b_false = qi.t0hi[k] >= c0lo_u || qi.t1hi[k] >= c1lo_u;
-        if (a_true || b_true) return 0;
-        if (!(a_false && b_false)) res = 2;
-    }
-    return res;
-}
 
 template <int DIM>
 __global__ void __launch_bounds__(128, MCLCCD_WALK_MIN_BLOCKS)
@@ -244,35 +192,6 @@ k_traverse_packet(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict
 // Stencil bits: VF a->b slot i = bit i, VF b->a slot i = bit 3+i,
 // EE (i,j) = bit 6 + 3i + j.
 // ---------------------------------------------------------------------------
-template <int DIM>
-__device__ __forceinline__ unsigned stencil_bits(const int *fa, const int *fb, unsigned ga, unsigned gb)
-{
-    unsigned bits = 0;
-#pragma unroll
-    for (int i = 0; i < DIM; ++i) {
-        bool sa = false, sb = false;
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) { sa |= fa[i] == fb[j]; sb |= fb[i] == fa[j]; }
-        if ((ga & (kFlagV0 << i)) && !sa) bits |= 1u << i;
-        if ((gb & (kFlagV0 << i)) && !sb) bits |= 1u << (3 + i);
-    }
-    if constexpr (DIM == 3) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            if (!(ga & (kFlagE0 << i))) continue;
-            const int a = fa[i], b = fa[(i + 1) % 3];
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                if (!(gb & (kFlagE0 << j))) continue;
-                const int c = fb[j], d = fb[(j + 1) % 3];
-                if (a == c || a == d || b == c || b == d) continue;
-                bits |= 1u << (6 + 3 * i + j);
-            }
-        }
-    }
-    return bits;
-}
-
 template <int DIM>
 __global__ void __launch_bounds__(256)
 k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, const int *__restrict__ P,
