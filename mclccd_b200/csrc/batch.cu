@@ -41,6 +41,11 @@
 
 namespace mclccd {
 
+// Scene's earliest hit key: toi bits, then k1 = (EE flag, v0, v1).
+struct __align__(16) BestKey {
+    unsigned long long toi, k1;
+};
+
 struct BatchRecord {
     int4 sten;
     double toi;
@@ -63,7 +68,8 @@ struct BatchGroupDev {
     const void *leaf_box;
     const unsigned char *leaf_active;
     unsigned long long *queue;
-    unsigned long long *n_hits, *min_toi, *n_disc, *n_sten, *done_ns;
+    unsigned long long *n_hits, *n_disc, *n_sten, *done_ns;
+    BestKey *best;
     BatchRecord *rec;
     unsigned long long *n_rec;
     unsigned long long rec_cap;
@@ -386,17 +392,45 @@ __device__ void batch_process(const BatchGroupDev &g, int m, const int2 *pairs, 
         }
         const int hs = hit ? sc : -1;
         scene_add(g.n_hits, hs, hit ? 1u : 0u);
-        if (hit) {
-            // the scene's earliest toi and the hits that set or tie it
-            const unsigned long long bits64 = (unsigned long long)__double_as_longlong(toi);
-            const unsigned long long cur = *(volatile unsigned long long *)(g.min_toi + sc);
-            if (bits64 <= cur) {
-                const unsigned long long old = atomicMin(g.min_toi + sc, bits64);
-                if (bits64 <= old) {
-                    const unsigned long long r = atomicAdd(g.n_rec, 1ull);
-                    if (r < g.rec_cap)
-                        g.rec[r] = BatchRecord{make_int4(s4[0], s4[1], s4[2], s4[3]), toi,
-                                               sc | (DIM == 3 ? kRecGroup3 : 0), vf ? 1 : 0};
+        // The scene's earliest hit under the order (toi, VF before EE, v0, v1,
+        // v2, v3): the lanes of one scene reduce to their smallest key, whose
+        // leader merges it into the scene's 16-byte (toi, k1) minimum with a
+        // compare-and-swap loop; hits that install or tie that minimum are
+        // logged with v2, v3 for the final choice among equal (toi, k1).
+        const unsigned long long kt = hit ? (unsigned long long)__double_as_longlong(toi) : ~0ull;
+        const unsigned long long k1 = hit ? ((unsigned long long)(vf ? 0 : 1) << 63) |
+                                                ((unsigned long long)(unsigned)s4[0] << 32) | (unsigned)s4[1]
+                                          : ~0ull;
+        const unsigned long long k2 = ((unsigned long long)(unsigned)s4[2] << 32) | (unsigned)s4[3];
+        const unsigned peers = __match_any_sync(kFull, hs);
+        unsigned long long bt = kt, b1 = k1, b2 = k2;
+        for (unsigned m = peers; m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            const unsigned long long ot = __shfl_sync(peers, kt, src), o1 = __shfl_sync(peers, k1, src),
+                                     o2 = __shfl_sync(peers, k2, src);
+            if (ot < bt || (ot == bt && (o1 < b1 || (o1 == b1 && o2 < b2)))) { bt = ot; b1 = o1; b2 = o2; }
+        }
+        if (hs >= 0 && lane == __ffs(peers) - 1 &&
+            bt <= *(volatile const unsigned long long *)&g.best[sc].toi) {
+            BestKey mine{bt, b1};
+            BestKey cur = atomicCAS(g.best + sc, BestKey{0ull, 0ull}, BestKey{0ull, 0ull});   // atomic read
+            bool keep = false;
+            for (int it = 0; it < 1024; ++it) {
+                if (cur.toi < mine.toi || (cur.toi == mine.toi && cur.k1 <= mine.k1)) {
+                    keep = cur.toi == mine.toi && cur.k1 == mine.k1;   // tie with the stored minimum
+                    break;
+                }
+                const BestKey prev = atomicCAS(g.best + sc, cur, mine);
+                if (prev.toi == cur.toi && prev.k1 == cur.k1) { keep = true; break; }
+                cur = prev;
+            }
+            if (keep) {
+                const unsigned long long r = atomicAdd(g.n_rec, 1ull);
+                if (r < g.rec_cap) {
+                    const double t = __longlong_as_double((long long)bt);
+                    const int v0 = (int)((b1 >> 32) & 0x7fffffffu), v1 = (int)(unsigned)b1;
+                    g.rec[r] = BatchRecord{make_int4(v0, v1, (int)(unsigned)(b2 >> 32), (int)(unsigned)b2), t,
+                                           sc | (DIM == 3 ? kRecGroup3 : 0), (b1 >> 63) ? 0 : 1};
                 }
             }
         }
@@ -432,8 +466,12 @@ struct FusedSmem {
     unsigned short code[W][kCodes];
 };
 
+#ifndef MCLCCD_BATCH_MIN_BLOCKS
+#define MCLCCD_BATCH_MIN_BLOCKS 2
+#endif
+
 template <int DIM, bool CERT, int BLOCK, int STACK>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, MCLCCD_BATCH_MIN_BLOCKS * 256 / BLOCK)
 k_batch_fused(BatchGroupDev g)
 {
     constexpr int S = DIM == 3 ? 3 : 2;
@@ -453,8 +491,7 @@ k_batch_fused(BatchGroupDev g)
     int q = -1, sc = 0, lq = 0, lb = 0, nb = 0, ns = 0, qprim = 0, node = 0, sp = 0, scan_k = 1, scan_end = 0;
     bool have_node = false, qact = true;
     long long steps = 0;
-    LeafBox<DIM> qb;
-    Box2T<DIM> qbox, qin;
+    Box2T<DIM> qbox;   // the query's FP32 boxes; its FP64 box is re-read on the rare undecided test
     unsigned long long next = 0, end = 0;
     bool drained = false;
 
@@ -467,14 +504,13 @@ k_batch_fused(BatchGroupDev g)
         lq = qi - lb;
         if (ns < 2 || lq >= ns - 1) return;   // nothing after it in its scene
         q = qi;
-        qb = lbox[qi];
+        const LeafBox<DIM> &qb = lbox[qi];
         qact = g.leaf_active[qi] != 0;
 #pragma unroll
         for (int k = 0; k < DIM; ++k) {
             qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
             qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
         }
-        qin = inner<DIM>(qbox);
         node = 0; sp = 0; have_node = true; scan_k = 1; scan_end = 0; steps = 0;
     };
 
@@ -517,16 +553,16 @@ k_batch_fused(BatchGroupDev g)
                     kbox.t0lo[d] = __double2float_rd(kb.lo0[d]); kbox.t0hi[d] = __double2float_ru(kb.hi0[d]);
                     kbox.t1lo[d] = __double2float_rd(kb.lo1[d]); kbox.t1hi[d] = __double2float_ru(kb.hi1[d]);
                 }
-                int r = leaf_test3<DIM>(qbox, qin, kbox);
-                if (r == 2) r = leaf_boxes_intersect<DIM>(qb, kb) ? 1 : 0;
+                int r = leaf_test3<DIM>(qbox, inner<DIM>(qbox), kbox);
+                if (r == 2) r = leaf_boxes_intersect<DIM>(lbox[q], kb) ? 1 : 0;
                 if (r == 1) {
                     const int kprim = __ldg(g.sorted + gk);
                     f[nf++] = make_int2(min(qprim, kprim), max(qprim, kprim));
                 }
             };
             auto test_child = [&](int c, const Box2T<DIM> &cb) {   // leaf child through its node box
-                int r = leaf_test3<DIM>(qbox, qin, cb);
-                if (r == 2) r = leaf_boxes_intersect<DIM>(qb, lbox[lb + c]) ? 1 : 0;
+                int r = leaf_test3<DIM>(qbox, inner<DIM>(qbox), cb);
+                if (r == 2) r = leaf_boxes_intersect<DIM>(lbox[q], lbox[lb + c]) ? 1 : 0;
                 if (r == 1) {
                     const int kprim = __ldg(g.sorted + lb + c);
                     f[nf++] = make_int2(min(qprim, kprim), max(qprim, kprim));
@@ -616,11 +652,13 @@ k_batch_fused(BatchGroupDev g)
     }
 }
 
-// Per-scene results: counts 0, earliest toi +inf.
-__global__ void k_b_init_results(unsigned long long *res, int n)
+// Per-scene results: counts 0, earliest-hit key (+inf, max).
+__global__ void k_b_init_results(unsigned long long *res, BestKey *best, int n)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 5 * n; i += gridDim.x * blockDim.x)
-        res[i] = (i / n) == 1 ? 0x7ff0000000000000ull : 0ull;   // min toi starts at +inf
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 5 * n; i += gridDim.x * blockDim.x) {
+        res[i] = 0ull;
+        if (i < n) best[i] = BestKey{0x7ff0000000000000ull, ~0ull};
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -643,7 +681,8 @@ struct GroupHost {
     unsigned *bounds = nullptr, *mort = nullptr, *keys = nullptr, *keys_alt = nullptr;
     void *sort_scratch = nullptr, *leaf_box = nullptr;
     Node *nodes = nullptr;
-    unsigned long long *res = nullptr;   // [5][n_scenes]: hits, min toi bits, discrete, stencils, done ns
+    unsigned long long *res = nullptr;   // [5][n_scenes]: hits, (unused), discrete, stencils, done ns
+    BestKey *best = nullptr;             // per scene: earliest-hit key
     unsigned long long *queue = nullptr;
     int grid = 0;                        // persistent grid of the current tuning
 };
@@ -812,8 +851,8 @@ cudaError_t enqueue_group(mclccd_batch *b, GroupHost &G, cudaStream_t st)
     g.V0 = G.V0; g.V1 = G.V1; g.P = G.P; g.flags = G.flags; g.prim_scene = G.prim_scene; g.sorted = G.vals;
     g.leaf_off = G.leaf_off; g.node_off = G.node_off; g.scene_np = G.scene_np; g.eta = G.eta;
     g.nodes = G.nodes; g.leaf_box = G.leaf_box; g.leaf_active = G.leaf_active; g.queue = G.queue;
-    g.n_hits = G.res; g.min_toi = G.res + G.n_scenes; g.n_disc = G.res + 2 * G.n_scenes;
-    g.n_sten = G.res + 3 * G.n_scenes; g.done_ns = G.res + 4 * G.n_scenes;
+    g.n_hits = G.res; g.n_disc = G.res + 2 * G.n_scenes;
+    g.n_sten = G.res + 3 * G.n_scenes; g.done_ns = G.res + 4 * G.n_scenes; g.best = G.best;
     g.rec = b->rec; g.n_rec = b->n_rec; g.rec_cap = b->rec_cap; g.err = err;
     g.chunk = b->tune[2]; g.leaf_size = b->tune[3];
     return fused(dim, b->precision == MCLCCD_PREC_FP32_CERTIFIED, g, b->tune[0], b->tune[1], st, false, G.grid);
@@ -826,7 +865,7 @@ cudaError_t enqueue_step(mclccd_batch *b, cudaStream_t st)
     cudaMemsetAsync(b->n_rec, 0, sizeof(unsigned long long), st);
     for (auto &G : b->grp) {
         if (G.n_scenes == 0) continue;
-        k_b_init_results<<<grid_of(5ll * G.n_scenes, 256, 64), 256, 0, st>>>(G.res, G.n_scenes);
+        k_b_init_results<<<grid_of(5ll * G.n_scenes, 256, 64), 256, 0, st>>>(G.res, G.best, G.n_scenes);
         cudaMemsetAsync(G.queue, 0, sizeof(unsigned long long), st);
     }
     for (auto &G : b->grp) {
@@ -973,6 +1012,7 @@ int mclccd_batch_set_scenes(mclccd_batch *b, int n_scenes, const int *scene_dim,
         MB_CUDA(b, balloc(b, G.leaf_active, np));
         MB_CUDA(b, balloc(b, G.flags, np));
         MB_CUDA(b, balloc(b, G.res, (size_t)G.n_scenes * 5));
+        MB_CUDA(b, balloc(b, G.best, (size_t)G.n_scenes));
         MB_CUDA(b, balloc(b, G.queue, 1));
         MB_CUDA(b, balloc(b, G.dst_off, G.n_scenes + 1));
         MB_CUDA(b, balloc(b, G.src_off, G.n_scenes));
@@ -1149,12 +1189,18 @@ int mclccd_batch_results(mclccd_batch *b, long long *n_hits, double *min_toi, in
         GroupHost &G = b->grp[gi];
         if (G.n_scenes == 0) continue;
         std::vector<unsigned long long> res((size_t)G.n_scenes * 5);
+        std::vector<BestKey> bk((size_t)G.n_scenes);
         MB_CUDA(b, cudaMemcpy(res.data(), G.res, sizeof(unsigned long long) * res.size(), cudaMemcpyDeviceToHost));
-        // argmin: among the logged hits with the scene's final toi, the
-        // smallest (VF before EE, then vertex ids)
+        MB_CUDA(b, cudaMemcpy(bk.data(), G.best, sizeof(BestKey) * bk.size(), cudaMemcpyDeviceToHost));
+        // argmin: the logged hit with the scene's final (toi, k1) and the
+        // smallest (v2, v3)
         std::vector<long long> best((size_t)G.n_scenes, -1);
-        auto key = [&](const BatchRecord &r) {
-            return std::make_tuple(r.is_vf ? 0 : 1, r.sten.x, r.sten.y, r.sten.z, r.sten.w);
+        auto k1_of = [](const BatchRecord &r) {
+            return ((unsigned long long)(r.is_vf ? 0 : 1) << 63) | ((unsigned long long)(unsigned)r.sten.x << 32) |
+                   (unsigned)r.sten.y;
+        };
+        auto k2_of = [](const BatchRecord &r) {
+            return ((unsigned long long)(unsigned)r.sten.z << 32) | (unsigned)r.sten.w;
         };
         for (size_t i = 0; i < rec.size(); ++i) {
             const BatchRecord &r = rec[i];
@@ -1163,13 +1209,13 @@ int mclccd_batch_results(mclccd_batch *b, long long *n_hits, double *min_toi, in
             if (rs >= G.n_scenes) continue;
             unsigned long long bits;
             std::memcpy(&bits, &r.toi, 8);
-            if (bits != res[(size_t)G.n_scenes + rs]) continue;
+            if (bits != bk[(size_t)rs].toi || k1_of(r) != bk[(size_t)rs].k1) continue;
             long long &cur = best[(size_t)rs];
-            if (cur < 0 || key(r) < key(rec[(size_t)cur])) cur = (long long)i;
+            if (cur < 0 || k2_of(r) < k2_of(rec[(size_t)cur])) cur = (long long)i;
         }
         for (int k = 0; k < G.n_scenes; ++k) {
             const int s = G.scene_user[k];
-            const unsigned long long mb = res[(size_t)G.n_scenes + k];
+            const unsigned long long mb = bk[(size_t)k].toi;
             double mt;
             std::memcpy(&mt, &mb, 8);
             if (n_hits) n_hits[s] = (long long)res[k];

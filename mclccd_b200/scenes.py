@@ -144,18 +144,18 @@ def annulus_2d(ring: int = 256, seed: int = 0, r_in: float = 0.3, r_out: float =
     rs = np.linspace(r_in, r_out, layers)
     th = np.arange(ring) * (2 * math.pi / ring)
     V = np.concatenate([np.stack([r * np.cos(th), r * np.sin(th)], 1) for r in rs])
-    tris = []
-    for l in range(layers - 1):
-        for i in range(ring):
-            a = l * ring + i
-            b = l * ring + (i + 1) % ring
-            c = a + ring
-            d = b + ring
-            tris.append((a, b, d))
-            tris.append((a, d, c))
-    T = np.array(tris, dtype=np.int64)
-    e = np.concatenate([T[:, [0, 1]], T[:, [1, 2]], T[:, [2, 0]]])
-    e = np.unique(np.sort(e, axis=1), axis=0)
+    l, i = np.meshgrid(np.arange(layers - 1), np.arange(ring), indexing="ij")
+    a = (l * ring + i).ravel()
+    b = (l * ring + (i + 1) % ring).ravel()
+    c = a + ring
+    d = b + ring
+    T = np.empty((2 * len(a), 3), dtype=np.int64)
+    T[0::2] = np.stack([a, b, d], axis=1)
+    T[1::2] = np.stack([a, d, c], axis=1)
+    e = np.sort(np.concatenate([T[:, [0, 1]], T[:, [1, 2]], T[:, [2, 0]]]), axis=1)
+    nvert = layers * ring
+    key = np.unique(e[:, 0] * nvert + e[:, 1])          # sorted unique edges, row-major (lo, hi)
+    e = np.stack([key // nvert, key % nvert], axis=1)
     ang = rng.uniform(-0.3, 0.3)
     R = np.array([[math.cos(ang), -math.sin(ang)], [math.sin(ang), math.cos(ang)]])
     shift = rng.normal(0.0, 0.05, 2)
