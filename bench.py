@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the certified/adjoint/batch form measurements")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-scene batch measurement")
     ap.add_argument("--tune", default="", help="launch knobs, e.g. walk_packet=0,accd_grid=2368")
     return ap.parse_args()
 
@@ -447,7 +448,44 @@ def measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev):
                       "forward_ms": f_ms, "backward_ms": b_ms, "backward_to_forward": b_ms / f_ms,
                       "hits": int(nh), "hits_with_gradient": int(res["v"][2])}
     del t3
+    if not args.no_batch:
+        out["batch"] = measure_batch(args)
     return out
+
+
+def measure_batch(args):
+    """Batching form: 512 scenes (384 folded cloths, side log-uniform in
+    [16, 384]; 128 2D annuli, ring resolution U[32, 2048]) per run, one CUDA
+    graph.  The autotuner picks the launch knobs on a 64-scene sample; the
+    full batch then runs once to capture and warm up, once timed."""
+    from mclccd_b200 import scenes
+    from mclccd_b200.autotune import tune_batch
+    from mclccd_b200.batch import Batch
+    sample = [s for _, s in scenes.batch_scenes(n3d=48, n2d=16, seed=1)]
+    tb = Batch()
+    tb.set_scenes(sample)
+    best, table = tune_batch(tb, space={"block": (128, 256), "stack": (64,), "chunk": (1, 4), "leaf": (1, 2)},
+                             repeats=1)
+    del tb, sample
+    full = [s for _, s in scenes.batch_scenes()]
+    tris = int(sum(len(s[2]) for s in full))
+    b = Batch()
+    b.set_scenes(full)
+    b.set_tuning(**best)
+    b.run()
+    b.results()
+    b.run()
+    r = b.results()
+    ms = r["batch_ms"]
+    d = r["done_ms"]
+    nst = int(r["n_stencils"].sum())
+    return {"workload": "512 scenes: 384 folded cloths (side log-uniform [16, 384], thickness 1e-3) + 128 2D "
+                        "annuli (ring U[32, 2048]), FP64, one CUDA graph per run",
+            "tris": tris, "batch_ms": ms, "scenes_per_s": 512 / ms * 1e3, "stencils": nst,
+            "stencils_per_s": nst / ms * 1e3, "hits": int(r["n_hits"].sum()),
+            "scene_latency_ms": {"p50": float(np.percentile(d, 50)), "p99": float(np.percentile(d, 99)),
+                                 "max": float(d.max())},
+            "tuning": best, "tuning_table": [[c, t] for c, t in table]}
 
 
 def main():

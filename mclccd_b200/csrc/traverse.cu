@@ -24,7 +24,7 @@ namespace mclccd {
 #define MCLCCD_WALK_STACK 64
 #endif
 #ifndef MCLCCD_WALK_MIN_BLOCKS
-#define MCLCCD_WALK_MIN_BLOCKS 1
+#define MCLCCD_WALK_MIN_BLOCKS 5
 #endif
 constexpr int kStackDepth = MCLCCD_WALK_STACK;
 
@@ -37,22 +37,25 @@ k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf
     constexpr int S = DIM == 3 ? 3 : 2;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n - 1) return;
-    const LeafBox<DIM> qb = leaf_box[q];
     const bool qact = leaf_active[q] != 0;
     const int qprim = sorted[q];
+    // Only the FP32 boxes stay in registers; the FP64 box is re-read for the
+    // rare undecided leaf test and the inner bracket recomputed per test.
     Box2T<DIM> qbox;
+    {
+        const LeafBox<DIM> &qb = leaf_box[q];
 #pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
-        qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
+        for (int k = 0; k < DIM; ++k) {
+            qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
+            qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
+        }
     }
-    const Box2T<DIM> qin = inner<DIM>(qbox);
 
     // Leaf k passed the cheap filters: decide it from the FP32 brackets and
     // fall back to the FP64 boxes only when they cannot tell.
     auto leaf = [&](int k, const Box2T<DIM> &kbox) {
-        int r = leaf_test3<DIM>(qbox, qin, kbox);
-        if (r == 2) r = leaf_boxes_intersect<DIM>(qb, leaf_box[k]) ? 1 : 0;
+        int r = leaf_test3<DIM>(qbox, inner<DIM>(qbox), kbox);
+        if (r == 2) r = leaf_boxes_intersect<DIM>(leaf_box[q], leaf_box[k]) ? 1 : 0;
         if (r == 1) {
             const int kprim = __ldg(sorted + k);
             unsigned long long slot = warp_append(&cnt->n_pairs);
