@@ -139,6 +139,29 @@ def algorithmic_bytes(c, n):
     return {"walk": walk, "expand": expand, "narrow": narrow, "refit": refit}
 
 
+def measured_traffic(c):
+    """DRAM bytes per stage of one step from the per-unit figures of the
+    committed ncu summary, scaled by this run's unit counts."""
+    per = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic_per_unit.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 2 and not line.startswith("#"):
+                    per[parts[0]] = float(parts[1])
+    except OSError:
+        return {}
+    out = {}
+    sten = c["vf"] + c["ee"]
+    if "walk_bytes_per_leaf_pair" in per:
+        out["walk"] = per["walk_bytes_per_leaf_pair"] * c["leaf_pairs"]
+    if "expand_bytes_per_stencil" in per:
+        out["expand"] = per["expand_bytes_per_stencil"] * sten
+    if "narrow_bytes_per_stencil" in per:
+        out["narrow"] = per["narrow_bytes_per_stencil"] * sten
+    return out
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -287,10 +310,15 @@ def run_b200(args, rank, world, local):
     top = max(kt, key=kt.get)
     peak, src = measured_peaks()
     achieved = ab[top] / (kt[top] / 1e3) / 1e9
+    tr = measured_traffic(c)
     roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": src,
+            "frac": achieved / peak, "traffic": tr.get(top), "peak_source": src,
+            "traffic_source": "ncu dram bytes per unit (profiles/dram_traffic_per_unit.txt) x this run's units",
             "algorithmic_bytes": ab[top], "kernel_ms": kt[top],
-            "all": {k: {"ms": kt[k], "GB/s": ab[k] / (kt[k] / 1e3) / 1e9 if kt[k] > 0 else None} for k in kt}}
+            "note": "narrow = the VF and EE ACCD launches of one step; they are FP64-pipe bound "
+                    "(56% of peak in profiles/walk_expand_accd_wavy385.md), their vertex gathers hit L2",
+            "all": {k: {"ms": kt[k], "GB/s": ab[k] / (kt[k] / 1e3) / 1e9 if kt[k] > 0 else None,
+                        "traffic": tr.get(k)} for k in kt}}
 
     # end to end through the C ABI from pinned host memory
     e2e = None
