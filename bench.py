@@ -37,7 +37,7 @@ METRIC = "CCD step ms & stencils/s at 2.1M tris: FP32-certified vs FP64 GPU vs T
 UNIT = "stencils/s"
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--no-forms", action="store_true", help="skip the certified/adjoint/batch form measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-scene batch measurement")
     ap.add_argument("--tune", default="", help="launch knobs, e.g. walk_packet=0,accd_grid=2368")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def dist_env():
@@ -169,6 +169,20 @@ def measured_peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def aggregate(dist, device, total_s, work):
+    """Whole-job figures over the ranks: the slowest rank's time and the
+    summed work (every rank takes the same two collective steps)."""
+    if dist is None:
+        return total_s, float(work)
+    import torch
+    t = torch.tensor([total_s, float(work)], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = t.clone()
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(tsum[1])
 
 
 def run_reference(args, rank, world):
@@ -299,13 +313,7 @@ def run_b200(args, rank, world, local):
     clk = clocks.stop()
     launches = tree.kernel_launches() - launches0
     total_s = sum(step_ms) / 1e3
-    if dist:
-        t = torch.tensor([total_s, float(sten)], dtype=torch.float64, device=dev)
-        tmax = t.clone(); dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone(); dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        total_max, sten_all = float(tmax[0]), float(tsum[1])
-    else:
-        total_max, sten_all = total_s, float(sten)
+    total_max, sten_all = aggregate(dist, dev, total_s, sten)
     value = sten_all / total_max
     c = tree.counts()
     pstats = tree.precision_stats()
@@ -358,12 +366,8 @@ def run_b200(args, rank, world, local):
                 e_ms.append(max(s0.elapsed_time(s1), wall))
                 h2d = V0.nbytes + V1a.nbytes + F.nbytes
                 d2h = cc["hits"] * (16 + 1 + 8) + cc["discrete"] * 8
-        e_total = sum(e_ms) / 1e3
-        if dist:
-            t = torch.tensor([e_total], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_total = float(t[0])
-        e2e = {"value": sten_all / e_total * (1.0 if True else 0), "unit": UNIT,
+        e_total, _ = aggregate(dist, dev, sum(e_ms) / 1e3, 0)
+        e2e = {"value": sten_all / e_total, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e_total * 1e3 / args.steps}
 
