@@ -139,3 +139,20 @@ def test_adjoint_status_cases():
     assert np.all(out["rows"][1:] == 0)
     ts, st, rows = Port().vjp_rows(V0, V1, sten, is_vf, toi, eta, eta)
     assert list(st) == [0, 1, 2]
+
+
+def test_autograd_function_backward_is_the_vjp():
+    torch = pytest.importorskip("torch")
+    from mclccd_b200.autograd import contact_toi
+    V0, V1, F, eta = scenes.folded_cloth(32, seed=8)
+    a0 = torch.tensor(V0, device="cuda", requires_grad=True)
+    a1 = torch.tensor(V1, device="cuda", requires_grad=True)
+    toi, sten, is_vf = contact_toi(a0, a1, torch.tensor(F, device="cuda"), eta)
+    w = torch.linspace(-1.0, 1.0, len(toi), dtype=torch.float64, device="cuda")
+    (toi * w).sum().backward()
+    out = vjp_toi(V0, V1, sten.cpu().numpy(), is_vf.cpu().numpy(), toi.detach().cpu().numpy(), w.cpu().numpy(),
+                  eta, eta)
+    g0, g1 = a0.grad.cpu().numpy(), a1.grad.cpu().numpy()
+    assert out["n_ok"] > 0
+    assert np.allclose(g0, out["dV0"], rtol=1e-12, atol=1e-12 * np.abs(g0).max())
+    assert np.allclose(g1, out["dV1"], rtol=1e-12, atol=1e-12 * np.abs(g1).max())
