@@ -241,6 +241,29 @@ int mclccd_batch_results(mclccd_batch *batch, long long *n_hits, double *min_toi
                          double *batch_ms);
 const char *mclccd_batch_last_error(const mclccd_batch *batch);
 
+/* Replaces: BVHTree::traverse(BVHTraverse<T,DIM>*) (BVHTree.hpp:96,
+ * BVHTree.cpp:162-166) through a device-side visitor (header-only
+ * include/mclccd_b200/visit.cuh).  Read-only view of the tree of the last
+ * update, valid until the next update or destroy (device memory):
+ *   nodes      n_leaves - 1 nodes of 128 B, root = node 0: float4 l[3], r[3]
+ *              = the left / right child's FP32 t0 and t1 boxes, outward
+ *              rounded (3D: l[0] = t0lo.xyz, t0hi.x; l[1] = t0hi.yz, t1lo.xy;
+ *              l[2] = t1lo.z, t1hi.xyz; 2D: l[0] = t0lo.xy, t0hi.xy;
+ *              l[1] = t1lo.xy, t1hi.xy), then int4 d = {split, meta, last,
+ *              parent}: the children are split and split + 1, each a leaf
+ *              (sorted index) if meta bit 0 (left) / bit 1 (right) is set,
+ *              else an internal node; last = the node's last leaf;
+ *   leaf_box   per sorted leaf the exact FP64 boxes lo0[dim], hi0[dim],
+ *              lo1[dim], hi1[dim] (t0 and t1, padded by box_eta);
+ *   leaf_prim  sorted leaf -> primitive index. */
+typedef struct {
+    int dim, n_leaves;
+    const void *nodes;
+    const double *leaf_box;
+    const int *leaf_prim;
+} mclccd_tree_view;
+int mclccd_get_tree_view(const mclccd_tree *tree, mclccd_tree_view *view);
+
 /* Per-stage device times (ms) of the last update + traverse when
  * MCLCCD_OPT_PROFILE is set: [update_total, build, refit, traverse_total,
  * tree_walk, expand, narrow]; returns how many were written. */

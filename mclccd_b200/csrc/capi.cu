@@ -806,6 +806,18 @@ int mclccd_precision_stats(const mclccd_tree *t, long long *n_fp64, long long *n
     return MCLCCD_OK;
 }
 
+int mclccd_get_tree_view(const mclccd_tree *t, mclccd_tree_view *view)
+{
+    if (!t || !view) return MCLCCD_ERR_INVALID;
+    if (!t->built || t->np < 1) return MCLCCD_ERR_STATE;
+    view->dim = t->dim;
+    view->n_leaves = t->np;
+    view->nodes = t->np > 1 ? t->nodes.p : nullptr;
+    view->leaf_box = static_cast<const double *>(t->leaf_box.p);
+    view->leaf_prim = static_cast<const int *>(t->vals.p);
+    return MCLCCD_OK;
+}
+
 int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)
 {
     if (!t || !ms || n < 0) return -1;
