@@ -208,7 +208,9 @@ int mclccd_tree_vjp_toi(mclccd_tree *tree, const double *g_toi, double *dV0, dou
  * eta[s] and the default options.  One mclccd_batch_run builds a segmented
  * LBVH over all scenes and runs one persistent traversal + narrow-phase kernel
  * with a global work queue, as a CUDA graph (captured on the first run after
- * the scenes, precision or tuning change, replayed afterwards).  Results are
+ * the scenes, precision or tuning change, replayed afterwards).  Traversal
+ * and narrow phase run in waves of queries inside that graph (a conditional
+ * WHILE node; a wave that overflows its buffers is redone smaller).  Results are
  * per-scene reductions rather than hit lists:
  *   n_hits, n_discrete, n_stencils  hits, discrete pairs and candidate
  *                                   stencils (VF + EE) of the scene;
@@ -221,9 +223,9 @@ int mclccd_tree_vjp_toi(mclccd_tree *tree, const double *g_toi, double *dV0, dou
  * V0/V1/P are the scenes' arrays concatenated in scene order (each scene's
  * own dim per row); P holds scene-local vertex ids. */
 typedef struct mclccd_batch mclccd_batch;
-#define MCLCCD_BATCH_TUNE_BLOCK 0   /* threads per block of the persistent kernel: 128 or 256 */
+#define MCLCCD_BATCH_TUNE_BLOCK 0   /* threads per block of the tree walk: 128 or 256 */
 #define MCLCCD_BATCH_TUNE_STACK 1   /* traversal stack entries per thread: 32 or 64 */
-#define MCLCCD_BATCH_TUNE_CHUNK 2   /* queries per lane taken from the work queue at a time: 1..64 */
+#define MCLCCD_BATCH_TUNE_CHUNK 2   /* wave buffer, in 2^20 leaf pairs (stencil buffers 2x VF, 4x EE): 1..64 */
 #define MCLCCD_BATCH_TUNE_LEAF 3    /* subtrees of up to this many leaves are scanned, not descended: 1..16 */
 #define MCLCCD_BATCH_TUNE_COUNT 4
 int mclccd_batch_create(mclccd_batch **out);

@@ -1,9 +1,9 @@
 """Autotuner for the launch knobs of the batched path (and the single-scene
 tree's grid sizes).
 
-``tune_batch`` times every configuration of the persistent kernel's
-compile-time shapes (threads per block, traversal stack depth) and run-time
-knobs (queue chunk, leaf-scan size) on the batch as it is set, checks that
+``tune_batch`` times every configuration of the batch walk's compile-time
+shapes (threads per block, traversal stack depth) and the run-time knobs
+(wave buffer size, leaf-scan size) on the batch as it is set, checks that
 every configuration gives the same per-scene results, and leaves the fastest
 one set.  A configuration whose stack overflows reports an error and is
 skipped.  Choices can be cached per GPU and workload signature in a JSON file.
@@ -18,7 +18,7 @@ import numpy as np
 
 from .ccd import CCDError
 
-DEFAULT_SPACE = {"block": (128, 256), "stack": (32, 64), "chunk": (1, 4, 16), "leaf": (1, 4)}
+DEFAULT_SPACE = {"block": (128, 256), "stack": (32, 64), "chunk": (8, 16, 32), "leaf": (1, 4)}
 
 
 def _signature(batch) -> str:

@@ -9,18 +9,19 @@
 // the scene, offset by the scene's base).  Refit is the usual bottom-up pass
 // with per-scene thickness.
 //
-// Traversal and narrow phase are one persistent kernel: warps pull query
-// leaves from a global counter in chunks, each lane walks one query through
-// its scene's tree (the exact leaf test of the single-scene path; pairs k > q
-// only, so each unordered pair once), and found leaf pairs go to a per-warp
-// shared-memory buffer.  Whenever 32 pairs are buffered the warp expands them
-// into stencils (VF first, then EE, so lanes run the same code path) and
-// evaluates ACCD on 32 stencils at a time, plus the discrete test per pair.
-// No stencil or hit list is materialised: per scene the kernel accumulates
-// candidate, hit and discrete counts, the earliest toi (atomicMin on its
-// bits) and the record-setting hits (a hit is logged when its toi is <= the
-// scene's minimum so far, so the scene's argmin is always among the logged
-// hits), and the time the scene's last work finished.
+// Traversal and narrow phase run in waves over the query leaves, all inside
+// one CUDA graph: a conditional WHILE node repeats one wave -- the walk of a
+// range of queries through their scenes' trees (the single-scene walk with
+// scene offsets; pairs k > q only, so each unordered pair once) into a
+// leaf-pair buffer, the single-scene stencil expansion (with the discrete
+// test), and ACCD over the VF and EE lists -- until every query is done.  A
+// device-side controller sizes the waves: a wave whose pairs or stencils
+// overflow their buffers is voided and redone with half the queries, and
+// waves that use under a quarter of the buffers double.  No hit list is
+// materialised: per scene the ACCD and discrete kernels accumulate candidate,
+// hit and discrete counts, the earliest hit (a 128-bit compare-and-swap on
+// its (toi, kind, v0, v1) key plus a log of ties), and the time the scene's
+// last work finished.
 //
 // Per-pair and per-stencil results are those of the single-scene path: same
 // leaf predicate, same canonical pair orientation, same stencil expansion and
@@ -67,14 +68,13 @@ struct BatchGroupDev {
     const Node *nodes;
     const void *leaf_box;
     const unsigned char *leaf_active;
-    unsigned long long *queue;
     unsigned long long *n_hits, *n_disc, *n_sten, *done_ns;
     BestKey *best;
     BatchRecord *rec;
     unsigned long long *n_rec;
     unsigned long long rec_cap;
     unsigned *err;
-    int chunk, leaf_size;
+    int leaf_size;
 };
 
 __device__ __forceinline__ unsigned long long global_ns()
@@ -272,14 +272,14 @@ __global__ void k_b_scatter(const double *__restrict__ src, double *__restrict__
 }
 
 // ---------------------------------------------------------------------------
-// Persistent traversal + narrow phase.
+// Waves: segmented walk -> stencil expansion -> ACCD with per-scene
+// reductions, repeated over the queries by a device-driven loop.
 // ---------------------------------------------------------------------------
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kPairBuf = 96;     // per warp: < 32 left over + up to 2 per lane per step
 constexpr int kScanFlag = 1 << 30;
 
 // Per-scene sums over the lanes of a warp that share a scene: one atomic per
-// scene and round.  All 32 lanes must call; scene < 0 contributes nothing.
+// scene.  All 32 lanes must call; scene < 0 contributes nothing.
 __device__ __forceinline__ void scene_add(unsigned long long *arr, int scene, unsigned v)
 {
     const unsigned peers = __match_any_sync(kFull, scene);
@@ -312,344 +312,290 @@ __device__ __forceinline__ int batch_accd(const int (&s)[4], bool vf, const Batc
     return hit;
 }
 
-// Expands and evaluates the first m (<= 32) buffered pairs of this warp.
-template <int DIM, bool CERT>
-__device__ void batch_process(const BatchGroupDev &g, int m, const int2 *pairs, int (*face)[2 * DIM], int *scn_of,
-                              unsigned short *codes)
+// The scene's earliest hit under the order (toi, VF before EE, v0, v1, v2,
+// v3): the lanes of one scene reduce to their smallest key, whose leader
+// merges it into the scene's 16-byte (toi, k1) minimum with a
+// compare-and-swap loop; hits that install or tie that minimum are logged
+// with v2, v3 for the final choice among equal (toi, k1).  All lanes call;
+// hs = the hit's scene or -1.
+template <int DIM>
+__device__ __forceinline__ void scene_best(const BatchGroupDev &g, int hs, double toi, const int (&s4)[4], bool vf)
 {
     const int lane = lane_id();
-    int fa[DIM], fb[DIM];
-    unsigned bits = 0;
-    int scene = -1;
-    bool disc = false;
-    if (lane < m) {
-        const int2 pr = pairs[lane];
-        scene = g.prim_scene[pr.x];
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) { fa[k] = __ldg(g.P + (size_t)pr.x * DIM + k); fb[k] = __ldg(g.P + (size_t)pr.y * DIM + k); }
-        bits = stencil_bits<DIM>(fa, fb, __ldg(g.flags + pr.x), __ldg(g.flags + pr.y));
-        bool shared = false, inb = true;
-#pragma unroll
-        for (int i = 0; i < DIM; ++i) {
-            inb = inb && fa[i] >= 0 && fa[i] < g.nv && fb[i] >= 0 && fb[i] < g.nv;
-#pragma unroll
-            for (int j = 0; j < DIM; ++j) shared |= fa[i] == fb[j];
+    const unsigned long long kt = hs >= 0 ? (unsigned long long)__double_as_longlong(toi) : ~0ull;
+    // cheap filter: only hits at or below the scene's current minimum contend
+    const bool cand = hs >= 0 && kt <= *(volatile const unsigned long long *)&g.best[hs].toi;
+    if (!__any_sync(kFull, cand)) return;
+    const int cs = cand ? hs : -1;
+    const unsigned long long k1 = cand ? ((unsigned long long)(vf ? 0 : 1) << 63) |
+                                             ((unsigned long long)(unsigned)s4[0] << 32) | (unsigned)s4[1]
+                                       : ~0ull;
+    const unsigned long long k2 = ((unsigned long long)(unsigned)s4[2] << 32) | (unsigned)s4[3];
+    const unsigned long long kc = cand ? kt : ~0ull;
+    const unsigned peers = __match_any_sync(kFull, cs);
+    unsigned long long bt = kc, b1 = k1, b2 = k2;
+    for (unsigned m = peers; m; m &= m - 1) {
+        const int src = __ffs(m) - 1;
+        const unsigned long long ot = __shfl_sync(peers, kc, src), o1 = __shfl_sync(peers, k1, src),
+                                 o2 = __shfl_sync(peers, k2, src);
+        if (ot < bt || (ot == bt && (o1 < b1 || (o1 == b1 && o2 < b2)))) { bt = ot; b1 = o1; b2 = o2; }
+    }
+    if (cs < 0 || lane != __ffs(peers) - 1) return;
+    BestKey mine{bt, b1};
+    BestKey cur = atomicCAS(g.best + cs, BestKey{0ull, 0ull}, BestKey{0ull, 0ull});   // atomic read
+    bool keep = false;
+    for (int it = 0; it < 1024; ++it) {
+        if (cur.toi < mine.toi || (cur.toi == mine.toi && cur.k1 <= mine.k1)) {
+            keep = cur.toi == mine.toi && cur.k1 == mine.k1;   // tie with the stored minimum
+            break;
         }
-        if (!inb) atomicOr(g.err, kErrBadIndex);
-        if (!shared && inb) {
-            double A[DIM][DIM], B[DIM][DIM];
+        const BestKey prev = atomicCAS(g.best + cs, cur, mine);
+        if (prev.toi == cur.toi && prev.k1 == cur.k1) { keep = true; break; }
+        cur = prev;
+    }
+    if (keep) {
+        const unsigned long long r = atomicAdd(g.n_rec, 1ull);
+        if (r < g.rec_cap) {
+            const double t = __longlong_as_double((long long)bt);
+            const int v0 = (int)((b1 >> 32) & 0x7fffffffu), v1 = (int)(unsigned)b1;
+            g.rec[r] = BatchRecord{make_int4(v0, v1, (int)(unsigned)(b2 >> 32), (int)(unsigned)b2), t,
+                                   cs | (DIM == 3 ? kRecGroup3 : 0), (b1 >> 63) ? 0 : 1};
+        }
+    }
+}
+
+// Device state of a group's wave loop.
+struct WaveState {
+    unsigned long long cursor;        // first query not yet done
+    unsigned long long q0, q1;        // this wave's queries
+    unsigned long long wave_q;        // queries per wave (adapted, kept across runs)
+    unsigned long long waves, redos;
+    unsigned long long used_pairs, used_vf, used_ee;
+    int redo, stop;
+};
+
+__global__ void k_wave_init(WaveState *ws, unsigned long long initial_q)
+{
+    ws->cursor = 0;
+    if (ws->wave_q == 0) ws->wave_q = initial_q;
+    ws->waves = ws->redos = 0;
+    ws->stop = 0;
+}
+
+__global__ void k_wave_begin(WaveState *ws, Counters *wc, unsigned long long n_total)
+{
+    wc->n_pairs = wc->n_vf = wc->n_ee = wc->n_discrete = 0;
+    ws->q0 = ws->cursor;
+    const unsigned long long q1 = ws->cursor + ws->wave_q;
+    ws->q1 = q1 < n_total ? q1 : n_total;
+    ws->redo = 0;
+}
+
+// Overflowed buffers void the wave (the next kernels then see zero work).
+__global__ void k_wave_check_pairs(WaveState *ws, Counters *wc, unsigned long long cap_pairs)
+{
+    ws->used_pairs = wc->n_pairs;
+    if (wc->n_pairs > cap_pairs) { ws->redo = 1; wc->n_pairs = 0; }
+}
+
+__global__ void k_wave_check_sten(WaveState *ws, Counters *wc, unsigned long long cap_vf, unsigned long long cap_ee,
+                                  unsigned long long cap_disc)
+{
+    ws->used_vf = wc->n_vf;
+    ws->used_ee = wc->n_ee;
+    if (ws->redo || wc->n_vf > cap_vf || wc->n_ee > cap_ee || wc->n_discrete > cap_disc) {
+        ws->redo = 1;
+        wc->n_vf = wc->n_ee = wc->n_discrete = 0;
+    }
+}
+
+// Advances the loop: a voided wave is redone with half the queries; a
+// done wave moves the cursor and may double the next wave.  Sets the loop
+// condition.  A single query that cannot fit, or a runaway loop, stops it
+// with an error.
+__global__ void k_wave_end(WaveState *ws, unsigned long long n_total, unsigned long long cap_pairs,
+                           unsigned long long cap_vf, unsigned long long cap_ee, cudaGraphConditionalHandle handle,
+                           unsigned *err)
+{
+    if (ws->redo) {
+        ++ws->redos;
+        if (ws->wave_q <= 1) { atomicOr(err, kErrWave); ws->stop = 1; }
+        else ws->wave_q >>= 1;
+    } else {
+        ws->cursor = ws->q1;
+        ++ws->waves;
+        if (4 * ws->used_pairs < cap_pairs && 4 * ws->used_vf < cap_vf && 4 * ws->used_ee < cap_ee &&
+            ws->wave_q < n_total)
+            ws->wave_q <<= 1;
+    }
+    if (ws->waves + ws->redos > (1ull << 24)) { atomicOr(err, kErrWave); ws->stop = 1; }
+    cudaGraphSetConditional(handle, (!ws->stop && ws->cursor < n_total) ? 1u : 0u);
+}
+
+// Walk of this wave's queries (one per thread, grid-stride), each in its
+// scene's tree: the single-scene walk with scene offsets, plus scanning
+// subtrees of at most leaf_size leaves instead of descending them.
+template <int DIM, int STACK>
+__global__ void __launch_bounds__(256)
+k_b_walk(BatchGroupDev g, const WaveState *ws, int2 *__restrict__ pairs, unsigned long long cap, Counters *wc)
+{
+    constexpr int S = DIM == 3 ? 3 : 2;
+    extern __shared__ int s_stack[];   // [STACK][blockDim.x]
+    const LeafBox<DIM> *lbox = reinterpret_cast<const LeafBox<DIM> *>(g.leaf_box);
+    const unsigned long long q0 = ws->q0, q1 = ws->q1;
+    const int tid = threadIdx.x, bs = blockDim.x;
+    for (unsigned long long qi = q0 + (unsigned long long)blockIdx.x * bs + tid; qi < q1;
+         qi += (unsigned long long)gridDim.x * bs) {
+        const int q = (int)qi;
+        const int qprim = g.sorted[q];
+        const int sc = g.prim_scene[qprim];
+        const int lb = g.leaf_off[sc], nb = g.node_off[sc], ns = g.scene_np[sc];
+        const int lq = q - lb;
+        if (ns < 2 || lq >= ns - 1) continue;
+        Box2T<DIM> qbox;
+        {
+            const LeafBox<DIM> &qb = lbox[q];
 #pragma unroll
-            for (int i = 0; i < DIM; ++i)
+            for (int k = 0; k < DIM; ++k) {
+                qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
+                qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
+            }
+        }
+        auto emit = [&](int k, int r) {   // local leaf k, three-valued test result r
+            if (r == 2) r = leaf_boxes_intersect<DIM>(lbox[q], lbox[lb + k]) ? 1 : 0;
+            if (r == 1) {
+                const int kprim = __ldg(g.sorted + lb + k);
+                const unsigned long long slot = warp_append(&wc->n_pairs);
+                if (slot < cap) pairs[slot] = make_int2(min(qprim, kprim), max(qprim, kprim));
+            }
+        };
+        auto test_leaf = [&](int k) {
+            const LeafBox<DIM> &kb = lbox[lb + k];
+            Box2T<DIM> kbox;
 #pragma unroll
-                for (int k = 0; k < DIM; ++k) {
-                    A[i][k] = __ldg(g.V1 + (size_t)fa[i] * DIM + k);
-                    B[i][k] = __ldg(g.V1 + (size_t)fb[i] * DIM + k);
+            for (int d = 0; d < DIM; ++d) {
+                kbox.t0lo[d] = __double2float_rd(kb.lo0[d]); kbox.t0hi[d] = __double2float_ru(kb.hi0[d]);
+                kbox.t1lo[d] = __double2float_rd(kb.lo1[d]); kbox.t1hi[d] = __double2float_ru(kb.hi1[d]);
+            }
+            emit(k, leaf_test3<DIM>(qbox, inner<DIM>(qbox), kbox));
+        };
+        int sp = 0, node = 0, scan_k = 1, scan_end = 0;
+        bool have_node = true;
+        for (long long steps = 0;; ++steps) {
+            if (steps > 4ll * ns + 64) { atomicOr(g.err, kErrStack); break; }
+            if (scan_k <= scan_end) { test_leaf(scan_k++); continue; }
+            if (!have_node) {
+                if (sp == 0) break;
+                const int e = s_stack[(--sp) * bs + tid];
+                if (e & kScanFlag) {
+                    const int c = e & ~kScanFlag;
+                    scan_k = max(__ldg(&g.nodes[nb + c].pad.x), lq + 1);
+                    scan_end = __ldg(&g.nodes[nb + c].d.z);
+                } else {
+                    node = e;
+                    have_node = true;
                 }
-            if constexpr (DIM == 3) disc = tri_tri(A[0], A[1], A[2], B[0], B[1], B[2]);
-            else disc = seg_seg(A[0], A[1], B[0], B[1]);
+                continue;
+            }
+            const Node *nd = g.nodes + nb + node;
+            float4 ls[S], rs[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) { ls[i] = __ldg(&nd->l[i]); rs[i] = __ldg(&nd->r[i]); }
+            const int4 d = __ldg(&nd->d);
+            const int first = __ldg(&nd->pad.x);
+            const int split = d.x, meta = d.y, last = d.z;
+            Box2T<DIM> lbx, rbx;
+            unpack_child<DIM>(ls, lbx);
+            unpack_child<DIM>(rs, rbx);
+            bool lok = split > lq, rok = last > lq;   // every batch leaf is active
+            if (lok && (meta & kMetaLeftLeaf)) { emit(split, leaf_test3<DIM>(qbox, inner<DIM>(qbox), lbx)); lok = false; }
+            if (rok && (meta & kMetaRightLeaf)) { emit(split + 1, leaf_test3<DIM>(qbox, inner<DIM>(qbox), rbx)); rok = false; }
+            lok = lok && boxes_may_intersect<DIM>(qbox, lbx);
+            rok = rok && boxes_may_intersect<DIM>(qbox, rbx);
+            const bool lscan = lok && split - first + 1 <= g.leaf_size;
+            const bool rscan = rok && last - split <= g.leaf_size;
+            have_node = false;
+            if (lok && rok) {
+                if (sp < STACK) s_stack[(sp++) * bs + tid] = rscan ? ((split + 1) | kScanFlag) : split + 1;
+                else { atomicOr(g.err, kErrStack); break; }
+            }
+            if (lok) {
+                if (lscan) { scan_k = max(first, lq + 1); scan_end = split; }
+                else { node = split; have_node = true; }
+            } else if (rok) {
+                if (rscan) { scan_k = max(split + 1, lq + 1); scan_end = last; }
+                else { node = split + 1; have_node = true; }
+            }
         }
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) { face[lane][k] = fa[k]; face[lane][DIM + k] = fb[k]; }
-        scn_of[lane] = scene;
     }
-    scene_add(g.n_sten, scene, __popc(bits));
-    scene_add(g.n_disc, scene, disc ? 1u : 0u);
-    // stencil codes (source lane << 4 | bit), VF first then EE
-    const unsigned nvf = __popc(bits & 0x3fu), nee = __popc(bits >> 6);
-    unsigned ivf = nvf, iee = nee;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned a = __shfl_up_sync(kFull, ivf, o), b = __shfl_up_sync(kFull, iee, o);
-        if (lane >= o) { ivf += a; iee += b; }
+}
+
+// Per-lane running sums for one scene, flushed (warp-aggregated) whenever a
+// lane's scene changes: the lists are scene-major, so flushes are rare.
+struct SceneSums {
+    int scene = -1;
+    unsigned a = 0, b = 0;
+    __device__ __forceinline__ void add(int sc, unsigned da, unsigned db, unsigned long long *A, unsigned long long *B,
+                                        unsigned long long *done_ns)
+    {
+        if (__any_sync(kFull, sc >= 0 && sc != scene)) flush(A, B, done_ns);
+        if (sc >= 0) { scene = sc; a += da; b += db; }
     }
-    const unsigned tvf = __shfl_sync(kFull, ivf, 31), tee = __shfl_sync(kFull, iee, 31);
-    unsigned pv = ivf - nvf, pe = tvf + iee - nee;
-    for (unsigned mm = bits & 0x3fu; mm; mm &= mm - 1) codes[pv++] = (unsigned short)((lane << 4) | (__ffs(mm) - 1));
-    for (unsigned mm = bits >> 6; mm; mm &= mm - 1) codes[pe++] = (unsigned short)((lane << 4) | (6 + __ffs(mm) - 1));
-    __syncwarp();
-    const unsigned total = tvf + tee;
-    for (unsigned base = 0; base < total; base += 32) {
-        const unsigned idx = base + lane;
+    __device__ __forceinline__ void flush(unsigned long long *A, unsigned long long *B, unsigned long long *done_ns)
+    {
+        scene_add(A, scene, a);
+        if (B) scene_add(B, scene, b);
+        scene_touch(done_ns, scene);
+        a = b = 0;
+    }
+};
+
+// ACCD over one stencil list of the wave, per-scene reductions.
+template <int DIM, bool VF, bool CERT>
+__global__ void __launch_bounds__(128, 4)
+k_b_accd(BatchGroupDev g, const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
+         const int *__restrict__ vert_scene)
+{
+    unsigned long long n = *(volatile const unsigned long long *)n_ptr;
+    if (n > cap) n = cap;
+    const int lane = lane_id();
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    SceneSums sums;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n;
+         base += stride) {
+        const unsigned long long i = base + lane;
+        int s4[4] = {-1, -1, -1, -1};
         int sc = -1;
         bool hit = false;
         double toi = -1.0;
-        int s4[4] = {-1, -1, -1, -1};
-        bool vf = true;
-        if (idx < total) {
-            const unsigned code = codes[idx];
-            const int pl = code >> 4, b = code & 15;
-            const int *A = face[pl], *B = face[pl] + DIM;
-            sc = scn_of[pl];
-            if (b < 6) {
-                const int *vs = b < 3 ? A : B, *fs = b < 3 ? B : A;
-                s4[0] = vs[b % 3]; s4[1] = fs[0]; s4[2] = fs[1]; s4[3] = DIM == 3 ? fs[DIM - 1] : -1;
-            } else {
-                const int i = (b - 6) / 3, j = (b - 6) % 3;
-                s4[0] = A[i]; s4[1] = A[(i + 1) % 3]; s4[2] = B[j]; s4[3] = B[(j + 1) % 3];
-                vf = false;
-            }
-            hit = batch_accd<DIM, CERT>(s4, vf, g, g.eta[sc], toi) && toi >= 0.0;
+        if (i < n) {
+            const int4 v = sten[i];
+            s4[0] = v.x; s4[1] = v.y; s4[2] = v.z; s4[3] = v.w;
+            sc = (v.x >= 0 && v.x < g.nv) ? vert_scene[v.x] : -1;
+            if (sc < 0) atomicOr(g.err, kErrBadIndex);
+            else hit = batch_accd<DIM, CERT>(s4, VF, g, g.eta[sc], toi) && toi >= 0.0;
         }
-        const int hs = hit ? sc : -1;
-        scene_add(g.n_hits, hs, hit ? 1u : 0u);
-        // The scene's earliest hit under the order (toi, VF before EE, v0, v1,
-        // v2, v3): the lanes of one scene reduce to their smallest key, whose
-        // leader merges it into the scene's 16-byte (toi, k1) minimum with a
-        // compare-and-swap loop; hits that install or tie that minimum are
-        // logged with v2, v3 for the final choice among equal (toi, k1).
-        const unsigned long long kt = hit ? (unsigned long long)__double_as_longlong(toi) : ~0ull;
-        const unsigned long long k1 = hit ? ((unsigned long long)(vf ? 0 : 1) << 63) |
-                                                ((unsigned long long)(unsigned)s4[0] << 32) | (unsigned)s4[1]
-                                          : ~0ull;
-        const unsigned long long k2 = ((unsigned long long)(unsigned)s4[2] << 32) | (unsigned)s4[3];
-        const unsigned peers = __match_any_sync(kFull, hs);
-        unsigned long long bt = kt, b1 = k1, b2 = k2;
-        for (unsigned m = peers; m; m &= m - 1) {
-            const int src = __ffs(m) - 1;
-            const unsigned long long ot = __shfl_sync(peers, kt, src), o1 = __shfl_sync(peers, k1, src),
-                                     o2 = __shfl_sync(peers, k2, src);
-            if (ot < bt || (ot == bt && (o1 < b1 || (o1 == b1 && o2 < b2)))) { bt = ot; b1 = o1; b2 = o2; }
-        }
-        if (hs >= 0 && lane == __ffs(peers) - 1 &&
-            bt <= *(volatile const unsigned long long *)&g.best[sc].toi) {
-            BestKey mine{bt, b1};
-            BestKey cur = atomicCAS(g.best + sc, BestKey{0ull, 0ull}, BestKey{0ull, 0ull});   // atomic read
-            bool keep = false;
-            for (int it = 0; it < 1024; ++it) {
-                if (cur.toi < mine.toi || (cur.toi == mine.toi && cur.k1 <= mine.k1)) {
-                    keep = cur.toi == mine.toi && cur.k1 == mine.k1;   // tie with the stored minimum
-                    break;
-                }
-                const BestKey prev = atomicCAS(g.best + sc, cur, mine);
-                if (prev.toi == cur.toi && prev.k1 == cur.k1) { keep = true; break; }
-                cur = prev;
-            }
-            if (keep) {
-                const unsigned long long r = atomicAdd(g.n_rec, 1ull);
-                if (r < g.rec_cap) {
-                    const double t = __longlong_as_double((long long)bt);
-                    const int v0 = (int)((b1 >> 32) & 0x7fffffffu), v1 = (int)(unsigned)b1;
-                    g.rec[r] = BatchRecord{make_int4(v0, v1, (int)(unsigned)(b2 >> 32), (int)(unsigned)b2), t,
-                                           sc | (DIM == 3 ? kRecGroup3 : 0), (b1 >> 63) ? 0 : 1};
-                }
-            }
-        }
+        sums.add(sc, sc >= 0 ? 1u : 0u, hit ? 1u : 0u, g.n_sten, g.n_hits, g.done_ns);
+        scene_best<DIM>(g, hit ? sc : -1, toi, s4, VF);
     }
-    scene_touch(g.done_ns, scene);
-    __syncwarp();
+    sums.flush(g.n_sten, g.n_hits, g.done_ns);
 }
 
-// Drops the first m entries of a warp's pair buffer (n <= kPairBuf entries).
-__device__ __forceinline__ void shift_pairs(int2 *buf, int m, int n)
+// Discrete pairs of the wave -> per-scene counts.
+__global__ void __launch_bounds__(256)
+k_b_disc(BatchGroupDev g, const int2 *__restrict__ disc, const unsigned long long *n_ptr, unsigned long long cap)
 {
-    const int lane = lane_id(), rem = n - m;
-    int2 a = make_int2(0, 0), b = make_int2(0, 0);
-    if (lane < rem) a = buf[m + lane];
-    if (lane + 32 < rem) b = buf[m + 32 + lane];
-    __syncwarp();
-    if (lane < rem) buf[lane] = a;
-    if (lane + 32 < rem) buf[32 + lane] = b;
-    __syncwarp();
-}
-
-// Dynamic shared memory of the persistent kernel: per-thread traversal
-// stacks, then per warp the pair buffer, the faces and scenes of the pairs
-// being expanded and their stencil codes.
-template <int DIM, int BLOCK, int STACK>
-struct FusedSmem {
-    static constexpr int W = BLOCK / 32;
-    static constexpr int kCodes = 32 * (DIM == 3 ? 15 : 6);
-    int stack[STACK][BLOCK];
-    int2 pairs[W][kPairBuf];
-    int face[W][32][2 * DIM];
-    int scene[W][32];
-    unsigned short code[W][kCodes];
-};
-
-#ifndef MCLCCD_BATCH_MIN_BLOCKS
-#define MCLCCD_BATCH_MIN_BLOCKS 2
-#endif
-
-template <int DIM, bool CERT, int BLOCK, int STACK>
-__global__ void __launch_bounds__(BLOCK, MCLCCD_BATCH_MIN_BLOCKS * 256 / BLOCK)
-k_batch_fused(BatchGroupDev g)
-{
-    constexpr int S = DIM == 3 ? 3 : 2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto &sm = *reinterpret_cast<FusedSmem<DIM, BLOCK, STACK> *>(smem_raw);
-    auto &s_stack = sm.stack;
-    auto &s_pairs = sm.pairs;
-    auto &s_face = sm.face;
-    auto &s_scene = sm.scene;
-    auto &s_code = sm.code;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const LeafBox<DIM> *lbox = reinterpret_cast<const LeafBox<DIM> *>(g.leaf_box);
-    const unsigned long long total = (unsigned long long)g.np;
-
-    int npairs = 0;
-    // query state of this lane
-    int q = -1, sc = 0, lq = 0, lb = 0, nb = 0, ns = 0, qprim = 0, node = 0, sp = 0, scan_k = 1, scan_end = 0;
-    bool have_node = false, qact = true;
-    long long steps = 0;
-    Box2T<DIM> qbox;   // the query's FP32 boxes; its FP64 box is re-read on the rare undecided test
-    unsigned long long next = 0, end = 0;
-    bool drained = false;
-
-    auto start_query = [&](int qi) {
-        qprim = g.sorted[qi];
-        sc = g.prim_scene[qprim];
-        lb = g.leaf_off[sc];
-        nb = g.node_off[sc];
-        ns = g.scene_np[sc];
-        lq = qi - lb;
-        if (ns < 2 || lq >= ns - 1) return;   // nothing after it in its scene
-        q = qi;
-        const LeafBox<DIM> &qb = lbox[qi];
-        qact = g.leaf_active[qi] != 0;
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) {
-            qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
-            qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
-        }
-        node = 0; sp = 0; have_node = true; scan_k = 1; scan_end = 0; steps = 0;
-    };
-
-    for (;;) {
-        // 1. idle lanes take the next queries of the warp's chunk
-        bool need = q < 0;
-        unsigned needm = __ballot_sync(kFull, need);
-        while (needm && !drained) {
-            if (next >= end) {
-                unsigned long long b0 = 0;
-                if (lane == 0) b0 = atomicAdd(g.queue, 32ull * (unsigned long long)g.chunk);
-                b0 = __shfl_sync(kFull, b0, 0);
-                if (b0 >= total) { drained = true; break; }
-                next = b0;
-                end = b0 + 32ull * (unsigned long long)g.chunk;
-                if (end > total) end = total;
-            }
-            const unsigned rank = __popc(needm & lanemask_lt());
-            const unsigned long long left = end - next, want = (unsigned long long)__popc(needm);
-            const unsigned take = (unsigned)(left < want ? left : want);
-            if (need && rank < take) { start_query((int)(next + rank)); need = false; }
-            next += take;
-            needm = __ballot_sync(kFull, need);
-        }
-        if (!__any_sync(kFull, q >= 0)) {
-            if (drained) break;
-            continue;   // every new query was trivial: take more
-        }
-        // 2. one unit of work per active lane: a scanned leaf or a node visit
-        int2 f[2];
-        int nf = 0;
-        int finished = -1;   // scene of a query that ends in this step
-        if (q >= 0) {
-            auto test_leaf = [&](int k) {   // k: local leaf index > lq
-                const int gk = lb + k;
-                const LeafBox<DIM> &kb = lbox[gk];
-                Box2T<DIM> kbox;
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    kbox.t0lo[d] = __double2float_rd(kb.lo0[d]); kbox.t0hi[d] = __double2float_ru(kb.hi0[d]);
-                    kbox.t1lo[d] = __double2float_rd(kb.lo1[d]); kbox.t1hi[d] = __double2float_ru(kb.hi1[d]);
-                }
-                int r = leaf_test3<DIM>(qbox, inner<DIM>(qbox), kbox);
-                if (r == 2) r = leaf_boxes_intersect<DIM>(lbox[q], kb) ? 1 : 0;
-                if (r == 1) {
-                    const int kprim = __ldg(g.sorted + gk);
-                    f[nf++] = make_int2(min(qprim, kprim), max(qprim, kprim));
-                }
-            };
-            auto test_child = [&](int c, const Box2T<DIM> &cb) {   // leaf child through its node box
-                int r = leaf_test3<DIM>(qbox, inner<DIM>(qbox), cb);
-                if (r == 2) r = leaf_boxes_intersect<DIM>(lbox[q], lbox[lb + c]) ? 1 : 0;
-                if (r == 1) {
-                    const int kprim = __ldg(g.sorted + lb + c);
-                    f[nf++] = make_int2(min(qprim, kprim), max(qprim, kprim));
-                }
-            };
-            if (++steps > 4ll * ns + 64) {
-                atomicOr(g.err, kErrStack);
-                q = -1;
-            } else if (scan_k <= scan_end) {
-                const int k = scan_k++;
-                test_leaf(k);
-            } else if (!have_node) {
-                if (sp == 0) {
-                    q = -1;   // query done
-                } else {
-                    const int e = s_stack[--sp][tid];
-                    if (e & kScanFlag) {
-                        const int c = e & ~kScanFlag;
-                        const int4 pd = __ldg(&g.nodes[nb + c].pad);
-                        const int4 dd = __ldg(&g.nodes[nb + c].d);
-                        scan_k = max(pd.x, lq + 1);
-                        scan_end = dd.z;
-                    } else {
-                        node = e;
-                        have_node = true;
-                    }
-                }
-            } else {
-                const Node *nd = g.nodes + nb + node;
-                float4 ls[S], rs[S];
-#pragma unroll
-                for (int i = 0; i < S; ++i) { ls[i] = __ldg(&nd->l[i]); rs[i] = __ldg(&nd->r[i]); }
-                const int4 d = __ldg(&nd->d);
-                const int first = __ldg(&nd->pad.x);
-                const int split = d.x, meta = d.y, last = d.z;
-                Box2T<DIM> lbx, rbx;
-                unpack_child<DIM>(ls, lbx);
-                unpack_child<DIM>(rs, rbx);
-                const bool lact = ((meta >> 8) & 0xff) != 0, ract = ((meta >> 16) & 0xff) != 0;
-                bool lok = split > lq && (qact || lact);
-                bool rok = last > lq && (qact || ract);
-                if (lok && (meta & kMetaLeftLeaf)) { test_child(split, lbx); lok = false; }
-                if (rok && (meta & kMetaRightLeaf)) { test_child(split + 1, rbx); rok = false; }
-                lok = lok && boxes_may_intersect<DIM>(qbox, lbx);
-                rok = rok && boxes_may_intersect<DIM>(qbox, rbx);
-                // small subtrees are scanned leaf by leaf instead of descended
-                const bool lscan = lok && split - first + 1 <= g.leaf_size;
-                const bool rscan = rok && last - split <= g.leaf_size;
-                have_node = false;
-                if (lok && rok) {
-                    if (sp < STACK) s_stack[sp++][tid] = rscan ? ((split + 1) | kScanFlag) : split + 1;
-                    else { atomicOr(g.err, kErrStack); q = -1; }
-                }
-                if (lok) {
-                    if (lscan) { scan_k = max(first, lq + 1); scan_end = split; }
-                    else { node = split; have_node = true; }
-                } else if (rok) {
-                    if (rscan) { scan_k = max(split + 1, lq + 1); scan_end = last; }
-                    else { node = split + 1; have_node = true; }
-                }
-            }
-            if (q < 0) finished = sc;
-        }
-        scene_touch(g.done_ns, finished);
-        // 3. buffer the found pairs
-        unsigned incl = nf;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned v = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += v;
-        }
-        const int tot = (int)__shfl_sync(kFull, incl, 31);
-        for (int j = 0; j < nf; ++j) s_pairs[warp][npairs + (int)(incl - nf) + j] = f[j];
-        npairs += tot;
-        __syncwarp();
-        while (npairs >= 32) {   // leaves < 32, so the next step's <= 64 pairs fit
-            batch_process<DIM, CERT>(g, 32, s_pairs[warp], s_face[warp], s_scene[warp], s_code[warp]);
-            shift_pairs(s_pairs[warp], 32, npairs);
-            npairs -= 32;
-        }
+    unsigned long long n = *(volatile const unsigned long long *)n_ptr;
+    if (n > cap) n = cap;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    SceneSums sums;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n;
+         base += stride) {
+        const unsigned long long i = base + lane_id();
+        const int sc = i < n ? g.prim_scene[disc[i].x] : -1;
+        sums.add(sc, sc >= 0 ? 1u : 0u, 0u, g.n_disc, nullptr, g.done_ns);
     }
-    while (npairs > 0) {
-        const int m = npairs < 32 ? npairs : 32;
-        batch_process<DIM, CERT>(g, m, s_pairs[warp], s_face[warp], s_scene[warp], s_code[warp]);
-        shift_pairs(s_pairs[warp], m, npairs);
-        npairs -= m;
-    }
+    sums.flush(g.n_disc, nullptr, g.done_ns);
 }
 
 // Per-scene results: counts 0, earliest-hit key (+inf, max).
@@ -683,8 +629,14 @@ struct GroupHost {
     Node *nodes = nullptr;
     unsigned long long *res = nullptr;   // [5][n_scenes]: hits, (unused), discrete, stencils, done ns
     BestKey *best = nullptr;             // per scene: earliest-hit key
-    unsigned long long *queue = nullptr;
-    int grid = 0;                        // persistent grid of the current tuning
+    int *vert_scene = nullptr;           // group scene of each group vertex
+    // wave buffers (sized by the wave-buffer tuning) and loop state
+    unsigned long long cap_pairs = 0, cap_vf = 0, cap_ee = 0, cap_disc = 0;
+    int2 *w_pairs = nullptr, *w_disc = nullptr;
+    int4 *w_vf = nullptr, *w_ee = nullptr;
+    Counters *w_cnt = nullptr;
+    WaveState *ws = nullptr;
+    cudaGraphConditionalHandle handle = 0;
 };
 
 int bits_for(int n)
@@ -703,7 +655,8 @@ using namespace mclccd;
 struct mclccd_batch {
     int device = 0;
     int precision = MCLCCD_PREC_FP64;
-    int tune[4] = {128, 64, 4, 1};   // block, stack, queue chunk, leaf size
+    int tune[4] = {128, 64, 16, 1};  // walk block size, walk stack, wave buffer (2^20 leaf pairs), leaf-scan size
+    int wave_chunk = 0;              // wave-buffer size the wave buffers were allocated for
     int n_scenes = 0;
     long long total_doubles = 0;
     std::vector<int> scene_dim;
@@ -750,6 +703,7 @@ void free_all(mclccd_batch *b)
     b->stage0 = b->stage1 = nullptr;
     b->n_scenes = 0;
     b->ran = false;
+    b->wave_chunk = 0;
 }
 
 int bfail(mclccd_batch *b, int code, const std::string &msg)
@@ -772,47 +726,36 @@ int grid_of(long long n, int block, int cap)
     return (int)std::max<long long>(1, std::min<long long>(g, cap));
 }
 
-// prepare = true: set the shared-memory limit and return the persistent grid
-// (outside graph capture); prepare = false: launch with that grid.
-template <int DIM, bool CERT, int BLOCK, int STACK>
-cudaError_t fused_t(const BatchGroupDev &g, cudaStream_t st, bool prepare, int &grid)
+template <int DIM, int STACK>
+cudaError_t walk_attr(int block)
 {
-    const size_t bytes = sizeof(FusedSmem<DIM, BLOCK, STACK>);
-    auto kern = k_batch_fused<DIM, CERT, BLOCK, STACK>;
-    if (prepare) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        if (e != cudaSuccess) return e;
-        int per_sm = 0, sms = 0, dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, bytes);
-        if (e != cudaSuccess) return e;
-        grid = std::max(1, per_sm) * std::max(1, sms);
-        return cudaSuccess;
-    }
-    kern<<<grid, BLOCK, bytes, st>>>(g);
-    return cudaGetLastError();
+    return cudaFuncSetAttribute(k_b_walk<DIM, STACK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                STACK * block * (int)sizeof(int));
 }
 
-template <int DIM, bool CERT>
-cudaError_t fused_d(const BatchGroupDev &g, int block, int stack, cudaStream_t st, bool prepare, int &grid)
+cudaError_t prepare_walk(int dim, int block, int stack)
 {
-    if (block == 256)
-        return stack == 32 ? fused_t<DIM, CERT, 256, 32>(g, st, prepare, grid) : fused_t<DIM, CERT, 256, 64>(g, st, prepare, grid);
-    return stack == 32 ? fused_t<DIM, CERT, 128, 32>(g, st, prepare, grid) : fused_t<DIM, CERT, 128, 64>(g, st, prepare, grid);
+    if (dim == 3) return stack == 32 ? walk_attr<3, 32>(block) : walk_attr<3, 64>(block);
+    return stack == 32 ? walk_attr<2, 32>(block) : walk_attr<2, 64>(block);
 }
 
-cudaError_t fused(int dim, bool cert, const BatchGroupDev &g, int block, int stack, cudaStream_t st, bool prepare,
-                  int &grid)
+BatchGroupDev group_view(mclccd_batch *b, GroupHost &G)
 {
-    if (dim == 3) return cert ? fused_d<3, true>(g, block, stack, st, prepare, grid) : fused_d<3, false>(g, block, stack, st, prepare, grid);
-    return cert ? fused_d<2, true>(g, block, stack, st, prepare, grid) : fused_d<2, false>(g, block, stack, st, prepare, grid);
+    BatchGroupDev g{};
+    g.np = G.np; g.nv = G.nv; g.n_scenes = G.n_scenes;
+    g.V0 = G.V0; g.V1 = G.V1; g.P = G.P; g.flags = G.flags; g.prim_scene = G.prim_scene; g.sorted = G.vals;
+    g.leaf_off = G.leaf_off; g.node_off = G.node_off; g.scene_np = G.scene_np; g.eta = G.eta;
+    g.nodes = G.nodes; g.leaf_box = G.leaf_box; g.leaf_active = G.leaf_active;
+    g.n_hits = G.res; g.n_disc = G.res + 2 * G.n_scenes;
+    g.n_sten = G.res + 3 * G.n_scenes; g.done_ns = G.res + 4 * G.n_scenes; g.best = G.best;
+    g.rec = b->rec; g.n_rec = b->n_rec; g.rec_cap = b->rec_cap; g.err = &b->cnt->err;
+    g.leaf_size = b->tune[MCLCCD_BATCH_TUNE_LEAF];
+    return g;
 }
 
-// Enqueues one full step (build + persistent traversal/narrow phase) of group g.
-cudaError_t enqueue_group(mclccd_batch *b, GroupHost &G, cudaStream_t st)
+// Segmented LBVH build of group G (before its wave loop).
+void enqueue_build(mclccd_batch *b, GroupHost &G, cudaStream_t st)
 {
-    if (G.np == 0) return cudaSuccess;
     const int dim = G.dim;
     unsigned *err = &b->cnt->err;
     const int gsz = grid_of(G.np, 256, 148 * 16);
@@ -846,33 +789,127 @@ cudaError_t enqueue_group(mclccd_batch *b, GroupHost &G, cudaStream_t st)
                                                          G.node_off, G.scene_np, G.eta, G.leaf_parent, G.nodes,
                                                          G.visits, reinterpret_cast<LeafBox<2> *>(G.leaf_box),
                                                          G.leaf_active, err);
-    BatchGroupDev g;
-    g.np = G.np; g.nv = G.nv; g.n_scenes = G.n_scenes;
-    g.V0 = G.V0; g.V1 = G.V1; g.P = G.P; g.flags = G.flags; g.prim_scene = G.prim_scene; g.sorted = G.vals;
-    g.leaf_off = G.leaf_off; g.node_off = G.node_off; g.scene_np = G.scene_np; g.eta = G.eta;
-    g.nodes = G.nodes; g.leaf_box = G.leaf_box; g.leaf_active = G.leaf_active; g.queue = G.queue;
-    g.n_hits = G.res; g.n_disc = G.res + 2 * G.n_scenes;
-    g.n_sten = G.res + 3 * G.n_scenes; g.done_ns = G.res + 4 * G.n_scenes; g.best = G.best;
-    g.rec = b->rec; g.n_rec = b->n_rec; g.rec_cap = b->rec_cap; g.err = err;
-    g.chunk = b->tune[2]; g.leaf_size = b->tune[3];
-    return fused(dim, b->precision == MCLCCD_PREC_FP32_CERTIFIED, g, b->tune[0], b->tune[1], st, false, G.grid);
 }
 
-cudaError_t enqueue_step(mclccd_batch *b, cudaStream_t st)
+template <int DIM, bool CERT>
+void enqueue_accd(const BatchGroupDev &g, GroupHost &G, cudaStream_t st)
 {
-    k_b_stamp<<<1, 1, 0, st>>>(b->t_start);
-    cudaMemsetAsync(b->cnt, 0, sizeof(Counters), st);
-    cudaMemsetAsync(b->n_rec, 0, sizeof(unsigned long long), st);
-    for (auto &G : b->grp) {
-        if (G.n_scenes == 0) continue;
-        k_b_init_results<<<grid_of(5ll * G.n_scenes, 256, 64), 256, 0, st>>>(G.res, G.best, G.n_scenes);
-        cudaMemsetAsync(G.queue, 0, sizeof(unsigned long long), st);
+    const int grid = 148 * 16;
+    k_b_accd<DIM, true, CERT><<<grid, 128, 0, st>>>(g, G.w_vf, &G.w_cnt->n_vf, G.cap_vf, G.vert_scene);
+    if constexpr (DIM == 3)
+        k_b_accd<DIM, false, CERT><<<grid, 128, 0, st>>>(g, G.w_ee, &G.w_cnt->n_ee, G.cap_ee, G.vert_scene);
+}
+
+// One wave: walk, expansion, ACCD, discrete counts, loop control.
+void enqueue_wave(mclccd_batch *b, GroupHost &G, cudaStream_t st)
+{
+    const BatchGroupDev g = group_view(b, G);
+    const int block = b->tune[MCLCCD_BATCH_TUNE_BLOCK], stack = b->tune[MCLCCD_BATCH_TUNE_STACK];
+    const unsigned long long nq = (unsigned long long)G.np;
+    k_wave_begin<<<1, 1, 0, st>>>(G.ws, G.w_cnt, nq);
+    const size_t smem = (size_t)stack * block * sizeof(int);
+    const int wgrid = 148 * (2048 / block);
+    if (G.dim == 3) {
+        if (stack == 32) k_b_walk<3, 32><<<wgrid, block, smem, st>>>(g, G.ws, G.w_pairs, G.cap_pairs, G.w_cnt);
+        else k_b_walk<3, 64><<<wgrid, block, smem, st>>>(g, G.ws, G.w_pairs, G.cap_pairs, G.w_cnt);
+    } else {
+        if (stack == 32) k_b_walk<2, 32><<<wgrid, block, smem, st>>>(g, G.ws, G.w_pairs, G.cap_pairs, G.w_cnt);
+        else k_b_walk<2, 64><<<wgrid, block, smem, st>>>(g, G.ws, G.w_pairs, G.cap_pairs, G.w_cnt);
     }
+    k_wave_check_pairs<<<1, 1, 0, st>>>(G.ws, G.w_cnt, G.cap_pairs);
+    launch_expand_pairs(G.dim, G.w_pairs, G.cap_pairs, G.P, G.flags, G.V1, G.nv, G.w_vf, G.cap_vf, G.w_ee, G.cap_ee,
+                        G.w_disc, G.cap_disc, 1, 1, G.w_cnt, 148 * 8, st);
+    k_wave_check_sten<<<1, 1, 0, st>>>(G.ws, G.w_cnt, G.cap_vf, G.cap_ee, G.cap_disc);
+    const bool cert = b->precision == MCLCCD_PREC_FP32_CERTIFIED;
+    if (G.dim == 3) { if (cert) enqueue_accd<3, true>(g, G, st); else enqueue_accd<3, false>(g, G, st); }
+    else { if (cert) enqueue_accd<2, true>(g, G, st); else enqueue_accd<2, false>(g, G, st); }
+    k_b_disc<<<148 * 4, 256, 0, st>>>(g, G.w_disc, &G.w_cnt->n_discrete, G.cap_disc);
+    k_wave_end<<<1, 1, 0, st>>>(G.ws, nq, G.cap_pairs, G.cap_vf, G.cap_ee, G.handle, &b->cnt->err);
+}
+
+// Whole step as a graph: build of each group, then its wave loop as a
+// conditional WHILE node whose body is one wave.
+cudaError_t capture_step(mclccd_batch *b, cudaGraph_t *out)
+{
+    cudaStream_t st = nullptr, body_st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&body_st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        k_b_stamp<<<1, 1, 0, st>>>(b->t_start);
+        cudaMemsetAsync(b->cnt, 0, sizeof(Counters), st);
+        cudaMemsetAsync(b->n_rec, 0, sizeof(unsigned long long), st);
+        for (auto &G : b->grp) {
+            if (G.n_scenes == 0) continue;
+            k_b_init_results<<<grid_of(5ll * G.n_scenes, 256, 64), 256, 0, st>>>(G.res, G.best, G.n_scenes);
+        }
+        for (auto &G : b->grp) {
+            if (G.np == 0 || e != cudaSuccess) continue;
+            enqueue_build(b, G, st);
+            k_wave_init<<<1, 1, 0, st>>>(G.ws, 1ull << 16);
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t graph = nullptr;
+            const cudaGraphNode_t *deps = nullptr;
+            size_t ndeps = 0;
+            e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps);
+            if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&G.handle, graph, 1, cudaGraphCondAssignDefault);
+            cudaGraphNodeParams cp = {};
+            cudaGraphNode_t node = nullptr;
+            if (e == cudaSuccess) {
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = G.handle;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
+            }
+            if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+            if (e == cudaSuccess)
+                e = cudaStreamBeginCaptureToGraph(body_st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                enqueue_wave(b, G, body_st);
+                cudaGraph_t body = nullptr;
+                e = cudaStreamEndCapture(body_st, &body);
+            }
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(st, &g);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) *out = g;
+        else if (g) cudaGraphDestroy(g);
+    }
+    if (body_st) cudaStreamDestroy(body_st);
+    if (st) cudaStreamDestroy(st);
+    return e;
+}
+
+// Wave buffers for the current wave-buffer tuning.
+cudaError_t ensure_wave_buffers(mclccd_batch *b)
+{
+    const int chunk = b->tune[MCLCCD_BATCH_TUNE_CHUNK];
+    if (b->wave_chunk == chunk) return cudaSuccess;
     for (auto &G : b->grp) {
-        cudaError_t e = enqueue_group(b, G, st);
+        for (void *p : {(void *)G.w_pairs, (void *)G.w_disc, (void *)G.w_vf, (void *)G.w_ee}) {
+            if (!p) continue;
+            cudaFree(p);
+            b->allocs.erase(std::remove(b->allocs.begin(), b->allocs.end(), p), b->allocs.end());
+        }
+        G.w_pairs = G.w_disc = nullptr;
+        G.w_vf = G.w_ee = nullptr;
+        if (G.np == 0) continue;
+        G.cap_pairs = (unsigned long long)chunk << 20;
+        G.cap_vf = 2 * G.cap_pairs;
+        G.cap_ee = G.dim == 3 ? 4 * G.cap_pairs : 0;
+        G.cap_disc = G.cap_pairs;
+        cudaError_t e = balloc(b, G.w_pairs, G.cap_pairs);
+        if (e == cudaSuccess) e = balloc(b, G.w_disc, G.cap_disc);
+        if (e == cudaSuccess) e = balloc(b, G.w_vf, G.cap_vf);
+        if (e == cudaSuccess && G.cap_ee) e = balloc(b, G.w_ee, G.cap_ee);
         if (e != cudaSuccess) return e;
     }
-    return cudaGetLastError();
+    b->wave_chunk = chunk;
+    return cudaSuccess;
 }
 
 } // namespace
@@ -990,6 +1027,9 @@ int mclccd_batch_set_scenes(mclccd_batch *b, int n_scenes, const int *scene_dim,
             for (int i = node_off[k]; i < node_off[k + 1]; ++i) nscene[(size_t)i] = k;
         }
         const size_t np = (size_t)np_tot, nv = (size_t)nv_tot, ni = (size_t)std::max<long long>(nint, 1);
+        std::vector<int> vscene(std::max<size_t>(nv, 1), 0);
+        for (int k = 0; k < G.n_scenes; ++k)
+            for (int i = 0; i < scene_nv[G.scene_user[k]]; ++i) vscene[(size_t)G.vbase[k] + i] = k;
         MB_CUDA(b, balloc(b, G.V0, nv * dim));
         MB_CUDA(b, balloc(b, G.V1, nv * dim));
         MB_CUDA(b, balloc(b, G.eta, G.n_scenes));
@@ -1013,7 +1053,10 @@ int mclccd_batch_set_scenes(mclccd_batch *b, int n_scenes, const int *scene_dim,
         MB_CUDA(b, balloc(b, G.flags, np));
         MB_CUDA(b, balloc(b, G.res, (size_t)G.n_scenes * 5));
         MB_CUDA(b, balloc(b, G.best, (size_t)G.n_scenes));
-        MB_CUDA(b, balloc(b, G.queue, 1));
+        MB_CUDA(b, balloc(b, G.vert_scene, std::max<size_t>(nv, 1)));
+        MB_CUDA(b, balloc(b, G.w_cnt, 1));
+        MB_CUDA(b, balloc(b, G.ws, 1));
+        MB_CUDA(b, cudaMemsetAsync(G.ws, 0, sizeof(WaveState), st));
         MB_CUDA(b, balloc(b, G.dst_off, G.n_scenes + 1));
         MB_CUDA(b, balloc(b, G.src_off, G.n_scenes));
         unsigned char *lb = nullptr;
@@ -1026,6 +1069,7 @@ int mclccd_batch_set_scenes(mclccd_batch *b, int n_scenes, const int *scene_dim,
         MB_CUDA(b, cudaMemcpyAsync(G.eta, heta.data(), sizeof(double) * G.n_scenes, cudaMemcpyHostToDevice, st));
         MB_CUDA(b, cudaMemcpyAsync(G.P, gP.data(), sizeof(int) * gP.size(), cudaMemcpyHostToDevice, st));
         MB_CUDA(b, cudaMemcpyAsync(G.prim_scene, pscene.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+        MB_CUDA(b, cudaMemcpyAsync(G.vert_scene, vscene.data(), sizeof(int) * vscene.size(), cudaMemcpyHostToDevice, st));
         MB_CUDA(b, cudaMemcpyAsync(G.leaf_off, leaf_off.data(), sizeof(int) * leaf_off.size(), cudaMemcpyHostToDevice, st));
         MB_CUDA(b, cudaMemcpyAsync(G.node_off, node_off.data(), sizeof(int) * node_off.size(), cudaMemcpyHostToDevice, st));
         MB_CUDA(b, cudaMemcpyAsync(G.scene_np, snp.data(), sizeof(int) * snp.size(), cudaMemcpyHostToDevice, st));
@@ -1127,26 +1171,16 @@ int mclccd_batch_run(mclccd_batch *b, void *stream)
         cudaEventDestroy(e);
     }
     if (b->dirty) {
-        for (auto &G : b->grp) {
-            if (G.np == 0) continue;
-            BatchGroupDev none{};
-            MB_CUDA(b, fused(G.dim, b->precision == MCLCCD_PREC_FP32_CERTIFIED, none, b->tune[0], b->tune[1], st, true,
-                             G.grid));
-        }
+        MB_CUDA(b, cudaStreamSynchronize(st));
+        MB_CUDA(b, ensure_wave_buffers(b));
+        for (auto &G : b->grp)
+            if (G.np > 0) MB_CUDA(b, prepare_walk(G.dim, b->tune[MCLCCD_BATCH_TUNE_BLOCK], b->tune[MCLCCD_BATCH_TUNE_STACK]));
         if (b->exec) cudaGraphExecDestroy(b->exec);
         if (b->graph) cudaGraphDestroy(b->graph);
         b->exec = nullptr;
         b->graph = nullptr;
-        cudaStream_t cap;
-        MB_CUDA(b, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            cudaError_t e2 = enqueue_step(b, cap);
-            e = cudaStreamEndCapture(cap, &b->graph);
-            if (e2 != cudaSuccess) e = e2;
-        }
+        cudaError_t e = capture_step(b, &b->graph);
         if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
-        cudaStreamDestroy(cap);
         if (e != cudaSuccess) { cudaGetLastError(); return bfail(b, MCLCCD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)); }
         b->dirty = false;
     }

@@ -23,6 +23,7 @@ constexpr unsigned kErrStack = 1u << 1;       // traversal stack overflow
 constexpr unsigned kErrSortWait = 1u << 2;    // radix-sort look-back gave up
 constexpr unsigned kErrHashFull = 1u << 3;    // edge hash table probe limit
 constexpr unsigned kErrAccdIters = 1u << 4;   // ACCD loop hit its 1000 cap (reported, result kept)
+constexpr unsigned kErrWave = 1u << 5;        // a batch wave could not fit its buffers
 
 // Device counters of one traverse: counts are exact even when a buffer is
 // too small (writes past capacity are skipped, the count keeps going).
