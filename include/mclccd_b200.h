@@ -206,11 +206,11 @@ int mclccd_tree_vjp_toi(mclccd_tree *tree, const double *g_toi, double *dV0, dou
  * Each scene is what one BVHTree<double, dim> would process (dim 2: P is an
  * edge list, dim 3: triangles), with box_eta = vf_ccd_eta = ee_ccd_eta =
  * eta[s] and the default options.  One mclccd_batch_run builds a segmented
- * LBVH over all scenes and runs one persistent traversal + narrow-phase kernel
- * with a global work queue, as a CUDA graph (captured on the first run after
- * the scenes, precision or tuning change, replayed afterwards).  Traversal
- * and narrow phase run in waves of queries inside that graph (a conditional
- * WHILE node; a wave that overflows its buffers is redone smaller).  Results are
+ * LBVH over all scenes, then traverses and scores them in one of two forms
+ * (MCLCCD_BATCH_TUNE_FORM below), as a CUDA graph (captured on the first run
+ * after the scenes, precision or tuning change, replayed afterwards).  In
+ * the waves form a wave that overflows its buffers is redone smaller inside
+ * the graph.  Results are
  * per-scene reductions rather than hit lists:
  *   n_hits, n_discrete, n_stencils  hits, discrete pairs and candidate
  *                                   stencils (VF + EE) of the scene;
@@ -223,11 +223,20 @@ int mclccd_tree_vjp_toi(mclccd_tree *tree, const double *g_toi, double *dV0, dou
  * V0/V1/P are the scenes' arrays concatenated in scene order (each scene's
  * own dim per row); P holds scene-local vertex ids. */
 typedef struct mclccd_batch mclccd_batch;
-#define MCLCCD_BATCH_TUNE_BLOCK 0   /* threads per block of the tree walk: 128 or 256 */
+#define MCLCCD_BATCH_TUNE_BLOCK 0   /* threads per block of the tree walk / persistent kernel: 128 or 256 */
 #define MCLCCD_BATCH_TUNE_STACK 1   /* traversal stack entries per thread: 32 or 64 */
-#define MCLCCD_BATCH_TUNE_CHUNK 2   /* wave buffer, in 2^20 leaf pairs (stencil buffers 2x VF, 4x EE): 1..64 */
+#define MCLCCD_BATCH_TUNE_CHUNK 2   /* persistent form: queries per lane a warp takes from the work queue: 1..64 */
 #define MCLCCD_BATCH_TUNE_LEAF 3    /* subtrees of up to this many leaves are scanned, not descended: 1..16 */
-#define MCLCCD_BATCH_TUNE_COUNT 4
+#define MCLCCD_BATCH_TUNE_FORM 4    /* MCLCCD_BATCH_FORM_WAVES (default) or MCLCCD_BATCH_FORM_PERSISTENT */
+#define MCLCCD_BATCH_TUNE_WAVE 5    /* waves form: wave buffer, in 2^16 leaf pairs (stencil buffers 2x VF, 4x EE): 1..1024 */
+#define MCLCCD_BATCH_TUNE_COUNT 6
+/* Forms of the batched step.  WAVES: per group, a device-driven loop of
+ * waves (walk -> stencil expansion -> ACCD -> per-scene reductions) in a
+ * conditional graph node.  PERSISTENT: per group, one persistent
+ * traversal-plus-narrow-phase kernel whose warps take query chunks from a
+ * global work queue.  Results are identical. */
+#define MCLCCD_BATCH_FORM_WAVES 0
+#define MCLCCD_BATCH_FORM_PERSISTENT 1
 int mclccd_batch_create(mclccd_batch **out);
 int mclccd_batch_destroy(mclccd_batch *batch);
 int mclccd_batch_set_scenes(mclccd_batch *batch, int n_scenes, const int *scene_dim, const int *scene_nv,
@@ -237,6 +246,9 @@ int mclccd_batch_set_positions(mclccd_batch *batch, const double *V0, const doub
 int mclccd_batch_set_precision(mclccd_batch *batch, int precision);
 int mclccd_batch_set_tuning(mclccd_batch *batch, int key, int value);
 int mclccd_batch_get_tuning(const mclccd_batch *batch, int key, int *value);
+/* Waves form: waves completed and waves redone smaller (buffer overflow) in
+ * the last run, summed over the 2D and 3D groups; 0, 0 in the persistent form. */
+int mclccd_batch_wave_stats(mclccd_batch *batch, long long *waves, long long *redos);
 int mclccd_batch_run(mclccd_batch *batch, void *stream);
 int mclccd_batch_results(mclccd_batch *batch, long long *n_hits, double *min_toi, int *min_sten,
                          unsigned char *min_is_vf, long long *n_discrete, long long *n_stencils, double *done_ms,

@@ -1,10 +1,12 @@
 """Autotuner for the launch knobs of the batched path (and the single-scene
 tree's grid sizes).
 
-``tune_batch`` times every configuration of the batch walk's compile-time
-shapes (threads per block, traversal stack depth) and the run-time knobs
-(wave buffer size, leaf-scan size) on the batch as it is set, checks that
-every configuration gives the same per-scene results, and leaves the fastest
+``tune_batch`` times every configuration of the batched step on the batch
+as it is set: the form (waves or persistent kernel), the compile-time shapes
+(threads per block, traversal stack depth) and the run-time knobs (leaf-scan
+size; the work-queue chunk of the persistent form, the wave buffer of the
+waves form; a knob the form does not use is not varied).  It checks that
+every configuration gives the same per-scene results and leaves the fastest
 one set.  A configuration whose stack overflows reports an error and is
 skipped.  Choices can be cached per GPU and workload signature in a JSON file.
 """
@@ -18,7 +20,10 @@ import numpy as np
 
 from .ccd import CCDError
 
-DEFAULT_SPACE = {"block": (128, 256), "stack": (32, 64), "chunk": (8, 16, 32), "leaf": (1, 4)}
+DEFAULT_SPACE = {"form": (0, 1), "block": (128, 256), "stack": (32, 64), "chunk": (1, 4, 16), "leaf": (1, 4),
+                 "wave": (256, 512, 1024)}
+# knobs that only one form reads
+_UNUSED = {0: ("chunk",), 1: ("wave",)}
 
 
 def _signature(batch) -> str:
@@ -39,8 +44,15 @@ def tune_batch(batch, space: dict | None = None, repeats: int = 3, cache: str | 
             return known[sig], []
     keys = list(space)
     table, ref, best, best_ms = [], None, None, float("inf")
+    seen = set()
     for vals in itertools.product(*(space[k] for k in keys)):
         cfg = dict(zip(keys, vals))
+        for k in _UNUSED.get(cfg.get("form"), ()):
+            if k in cfg:
+                cfg[k] = space[k][0]
+        if tuple(cfg.items()) in seen:
+            continue
+        seen.add(tuple(cfg.items()))
         try:
             batch.set_tuning(**cfg)
             ms = []

@@ -2,8 +2,12 @@
 
 Each scene is what one ``BVHTree(dim)`` would process with
 box_eta = vf_ccd_eta = ee_ccd_eta = eta.  One ``run`` is a CUDA graph: a
-segmented LBVH build over all scenes and one persistent traversal +
-narrow-phase kernel with a global work queue.  Results are per scene:
+segmented LBVH build over all scenes, then traversal and narrow phase in
+one of two forms (tuning key ``form``): ``FORM_WAVES``, a device-driven
+loop of waves (walk -> stencil expansion -> ACCD -> per-scene reductions)
+in a conditional graph node, or ``FORM_PERSISTENT``, one persistent
+traversal + narrow-phase kernel per group with a global work queue.  The
+results are identical; the autotuner picks the faster.  Results are per scene:
 hit / discrete / candidate counts, the earliest toi and its stencil, and
 the device time at which the scene's last work finished.
 """
@@ -15,7 +19,8 @@ import numpy as np
 
 from .ccd import OK, MEM_HOST, PREC_FP64, CCDError, lib
 
-TUNE_KEYS = {"block": 0, "stack": 1, "chunk": 2, "leaf": 3}
+TUNE_KEYS = {"block": 0, "stack": 1, "chunk": 2, "leaf": 3, "form": 4, "wave": 5}
+FORM_WAVES, FORM_PERSISTENT = 0, 1
 
 
 def _sig(L):
@@ -30,6 +35,7 @@ def _sig(L):
         "mclccd_batch_set_precision": ([vp, C.c_int], C.c_int),
         "mclccd_batch_set_tuning": ([vp, C.c_int, C.c_int], C.c_int),
         "mclccd_batch_get_tuning": ([vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "mclccd_batch_wave_stats": ([vp, llp, llp], C.c_int),
         "mclccd_batch_run": ([vp, vp], C.c_int),
         "mclccd_batch_results": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "mclccd_batch_last_error": ([vp], C.c_char_p),
@@ -84,6 +90,12 @@ class Batch:
             self._check(self._L.mclccd_batch_get_tuning(self._h, i, C.byref(v)), self._h)
             out[k] = v.value
         return out
+
+    def wave_stats(self):
+        """(waves, redos) of the last run in the waves form."""
+        w, r = C.c_longlong(), C.c_longlong()
+        self._check(self._L.mclccd_batch_wave_stats(self._h, C.byref(w), C.byref(r)), self._h)
+        return w.value, r.value
 
     def set_scenes(self, scenes):
         """scenes: sequence of (V0, V1, P, eta); V0/V1 nv x dim float64, P

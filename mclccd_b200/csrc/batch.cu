@@ -68,13 +68,14 @@ struct BatchGroupDev {
     const Node *nodes;
     const void *leaf_box;
     const unsigned char *leaf_active;
+    unsigned long long *queue;      // persistent form: next query to hand out
     unsigned long long *n_hits, *n_disc, *n_sten, *done_ns;
     BestKey *best;
     BatchRecord *rec;
     unsigned long long *n_rec;
     unsigned long long rec_cap;
     unsigned *err;
-    int leaf_size;
+    int chunk, leaf_size;
 };
 
 __device__ __forceinline__ unsigned long long global_ns()
@@ -598,6 +599,294 @@ k_b_disc(BatchGroupDev g, const int2 *__restrict__ disc, const unsigned long lon
     sums.flush(g.n_disc, nullptr, g.done_ns);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form: one kernel per group walks, expands and scores.  Warps
+// take chunks of queries from a global work queue; each lane walks its
+// query's scene tree one node (or scanned leaf) per step, found pairs go to a
+// per-warp shared-memory buffer, and every 32 buffered pairs the warp runs
+// the discrete tests, expands the stencils (VF first, then EE) and scores
+// them 32 at a time.  Nothing but per-scene results leaves the chip.
+// ---------------------------------------------------------------------------
+constexpr int kPairBuf = 96;   // per warp: < 32 left over + up to 2 per lane per step
+
+// Expands and evaluates the first m (<= 32) buffered pairs of this warp.
+template <int DIM, bool CERT>
+__device__ void batch_process(const BatchGroupDev &g, int m, const int2 *pairs, int (*face)[2 * DIM], int *scn_of,
+                              unsigned short *codes)
+{
+    const int lane = lane_id();
+    int fa[DIM], fb[DIM];
+    unsigned bits = 0;
+    int scene = -1;
+    bool disc = false;
+    if (lane < m) {
+        const int2 pr = pairs[lane];
+        scene = g.prim_scene[pr.x];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) { fa[k] = __ldg(g.P + (size_t)pr.x * DIM + k); fb[k] = __ldg(g.P + (size_t)pr.y * DIM + k); }
+        bits = stencil_bits<DIM>(fa, fb, __ldg(g.flags + pr.x), __ldg(g.flags + pr.y));
+        bool shared = false, inb = true;
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) {
+            inb = inb && fa[i] >= 0 && fa[i] < g.nv && fb[i] >= 0 && fb[i] < g.nv;
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) shared |= fa[i] == fb[j];
+        }
+        if (!inb) atomicOr(g.err, kErrBadIndex);
+        if (!shared && inb) {
+            double A[DIM][DIM], B[DIM][DIM];
+#pragma unroll
+            for (int i = 0; i < DIM; ++i)
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) {
+                    A[i][k] = __ldg(g.V1 + (size_t)fa[i] * DIM + k);
+                    B[i][k] = __ldg(g.V1 + (size_t)fb[i] * DIM + k);
+                }
+            if constexpr (DIM == 3) disc = tri_tri(A[0], A[1], A[2], B[0], B[1], B[2]);
+            else disc = seg_seg(A[0], A[1], B[0], B[1]);
+        }
+        if (!inb) bits = 0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) { face[lane][k] = fa[k]; face[lane][DIM + k] = fb[k]; }
+        scn_of[lane] = scene;
+    }
+    scene_add(g.n_sten, scene, __popc(bits));
+    scene_add(g.n_disc, scene, disc ? 1u : 0u);
+    // stencil codes (source lane << 4 | bit), VF first then EE
+    const unsigned nvf = __popc(bits & 0x3fu), nee = __popc(bits >> 6);
+    unsigned ivf = nvf, iee = nee;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned a = __shfl_up_sync(kFull, ivf, o), b = __shfl_up_sync(kFull, iee, o);
+        if (lane >= o) { ivf += a; iee += b; }
+    }
+    const unsigned tvf = __shfl_sync(kFull, ivf, 31), tee = __shfl_sync(kFull, iee, 31);
+    unsigned pv = ivf - nvf, pe = tvf + iee - nee;
+    for (unsigned mm = bits & 0x3fu; mm; mm &= mm - 1) codes[pv++] = (unsigned short)((lane << 4) | (__ffs(mm) - 1));
+    for (unsigned mm = bits >> 6; mm; mm &= mm - 1) codes[pe++] = (unsigned short)((lane << 4) | (6 + __ffs(mm) - 1));
+    __syncwarp();
+    const unsigned total = tvf + tee;
+    for (unsigned base = 0; base < total; base += 32) {
+        const unsigned idx = base + lane;
+        int sc = -1;
+        bool hit = false;
+        double toi = -1.0;
+        int s4[4] = {-1, -1, -1, -1};
+        bool vf = true;
+        if (idx < total) {
+            const unsigned code = codes[idx];
+            const int pl = code >> 4, b = code & 15;
+            const int *A = face[pl], *B = face[pl] + DIM;
+            sc = scn_of[pl];
+            if (b < 6) {
+                const int *vs = b < 3 ? A : B, *fs = b < 3 ? B : A;
+                s4[0] = vs[b % 3]; s4[1] = fs[0]; s4[2] = fs[1]; s4[3] = DIM == 3 ? fs[DIM - 1] : -1;
+            } else {
+                const int i = (b - 6) / 3, j = (b - 6) % 3;
+                s4[0] = A[i]; s4[1] = A[(i + 1) % 3]; s4[2] = B[j]; s4[3] = B[(j + 1) % 3];
+                vf = false;
+            }
+            hit = batch_accd<DIM, CERT>(s4, vf, g, g.eta[sc], toi) && toi >= 0.0;
+        }
+        const int hs = hit ? sc : -1;
+        scene_add(g.n_hits, hs, hit ? 1u : 0u);
+        scene_best<DIM>(g, hs, toi, s4, vf);
+    }
+    scene_touch(g.done_ns, scene);
+    __syncwarp();
+}
+
+// Drops the first m = 32 (or all) entries of a warp's pair buffer of n < kPairBuf.
+__device__ __forceinline__ void shift_pairs(int2 *buf, int m, int n)
+{
+    const int lane = lane_id(), rem = n - m;
+    int2 a = make_int2(0, 0), b = make_int2(0, 0);
+    if (lane < rem) a = buf[m + lane];
+    if (lane + 32 < rem) b = buf[m + 32 + lane];
+    __syncwarp();
+    if (lane < rem) buf[lane] = a;
+    if (lane + 32 < rem) buf[32 + lane] = b;
+    __syncwarp();
+}
+
+// Dynamic shared memory of the persistent kernel: per-thread traversal
+// stacks, then per warp the pair buffer, the faces and scenes of the pairs
+// being expanded and their stencil codes.
+template <int DIM, int BLOCK, int STACK>
+struct FusedSmem {
+    static constexpr int W = BLOCK / 32;
+    static constexpr int kCodes = 32 * (DIM == 3 ? 15 : 6);
+    int stack[STACK][BLOCK];
+    int2 pairs[W][kPairBuf];
+    int face[W][32][2 * DIM];
+    int scene[W][32];
+    unsigned short code[W][kCodes];
+};
+
+template <int DIM, bool CERT, int BLOCK, int STACK>
+__global__ void __launch_bounds__(BLOCK, 512 / BLOCK)
+k_batch_fused(BatchGroupDev g)
+{
+    constexpr int S = DIM == 3 ? 3 : 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto &sm = *reinterpret_cast<FusedSmem<DIM, BLOCK, STACK> *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const LeafBox<DIM> *lbox = reinterpret_cast<const LeafBox<DIM> *>(g.leaf_box);
+    const unsigned long long total = (unsigned long long)g.np;
+
+    int npairs = 0;
+    // query state of this lane
+    int q = -1, sc = 0, lq = 0, lb = 0, nb = 0, ns = 0, qprim = 0, node = 0, sp = 0, scan_k = 1, scan_end = 0;
+    bool have_node = false;
+    long long steps = 0;
+    Box2T<DIM> qbox;   // the query's FP32 boxes; its FP64 box is re-read on the rare undecided test
+    unsigned long long next = 0, end = 0;
+    bool drained = false;
+
+    auto start_query = [&](int qi) {
+        qprim = g.sorted[qi];
+        sc = g.prim_scene[qprim];
+        lb = g.leaf_off[sc];
+        nb = g.node_off[sc];
+        ns = g.scene_np[sc];
+        lq = qi - lb;
+        if (ns < 2 || lq >= ns - 1) return;   // nothing after it in its scene
+        q = qi;
+        const LeafBox<DIM> &qb = lbox[qi];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
+            qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
+        }
+        node = 0; sp = 0; have_node = true; scan_k = 1; scan_end = 0; steps = 0;
+    };
+
+    for (;;) {
+        // 1. idle lanes take the next queries of the warp's chunk
+        bool need = q < 0;
+        unsigned needm = __ballot_sync(kFull, need);
+        while (needm && !drained) {
+            if (next >= end) {
+                unsigned long long b0 = 0;
+                if (lane == 0) b0 = atomicAdd(g.queue, 32ull * (unsigned long long)g.chunk);
+                b0 = __shfl_sync(kFull, b0, 0);
+                if (b0 >= total) { drained = true; break; }
+                next = b0;
+                end = b0 + 32ull * (unsigned long long)g.chunk;
+                if (end > total) end = total;
+            }
+            const unsigned rank = __popc(needm & lanemask_lt());
+            const unsigned long long left = end - next, want = (unsigned long long)__popc(needm);
+            const unsigned take = (unsigned)(left < want ? left : want);
+            if (need && rank < take) { start_query((int)(next + rank)); need = false; }
+            next += take;
+            needm = __ballot_sync(kFull, need);
+        }
+        if (!__any_sync(kFull, q >= 0)) {
+            if (drained) break;
+            continue;   // every new query was trivial: take more
+        }
+        // 2. one unit of work per active lane: a scanned leaf or a node visit
+        int2 f[2];
+        int nf = 0;
+        int finished = -1;   // scene of a query that ends in this step
+        if (q >= 0) {
+            auto found = [&](int k, int r) {   // local leaf k, three-valued test result r
+                if (r == 2) r = leaf_boxes_intersect<DIM>(lbox[q], lbox[lb + k]) ? 1 : 0;
+                if (r == 1) {
+                    const int kprim = __ldg(g.sorted + lb + k);
+                    f[nf++] = make_int2(min(qprim, kprim), max(qprim, kprim));
+                }
+            };
+            if (++steps > 4ll * ns + 64) {
+                atomicOr(g.err, kErrStack);
+                q = -1;
+            } else if (scan_k <= scan_end) {
+                const int k = scan_k++;
+                const LeafBox<DIM> &kb = lbox[lb + k];
+                Box2T<DIM> kbox;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    kbox.t0lo[d] = __double2float_rd(kb.lo0[d]); kbox.t0hi[d] = __double2float_ru(kb.hi0[d]);
+                    kbox.t1lo[d] = __double2float_rd(kb.lo1[d]); kbox.t1hi[d] = __double2float_ru(kb.hi1[d]);
+                }
+                found(k, leaf_test3<DIM>(qbox, inner<DIM>(qbox), kbox));
+            } else if (!have_node) {
+                if (sp == 0) {
+                    q = -1;   // query done
+                } else {
+                    const int e = sm.stack[--sp][tid];
+                    if (e & kScanFlag) {
+                        const int c = e & ~kScanFlag;
+                        scan_k = max(__ldg(&g.nodes[nb + c].pad.x), lq + 1);
+                        scan_end = __ldg(&g.nodes[nb + c].d.z);
+                    } else {
+                        node = e;
+                        have_node = true;
+                    }
+                }
+            } else {
+                const Node *nd = g.nodes + nb + node;
+                float4 ls[S], rs[S];
+#pragma unroll
+                for (int i = 0; i < S; ++i) { ls[i] = __ldg(&nd->l[i]); rs[i] = __ldg(&nd->r[i]); }
+                const int4 d = __ldg(&nd->d);
+                const int first = __ldg(&nd->pad.x);
+                const int split = d.x, meta = d.y, last = d.z;
+                Box2T<DIM> lbx, rbx;
+                unpack_child<DIM>(ls, lbx);
+                unpack_child<DIM>(rs, rbx);
+                bool lok = split > lq, rok = last > lq;   // every batch leaf is active
+                if (lok && (meta & kMetaLeftLeaf)) { found(split, leaf_test3<DIM>(qbox, inner<DIM>(qbox), lbx)); lok = false; }
+                if (rok && (meta & kMetaRightLeaf)) { found(split + 1, leaf_test3<DIM>(qbox, inner<DIM>(qbox), rbx)); rok = false; }
+                lok = lok && boxes_may_intersect<DIM>(qbox, lbx);
+                rok = rok && boxes_may_intersect<DIM>(qbox, rbx);
+                // small subtrees are scanned leaf by leaf instead of descended
+                const bool lscan = lok && split - first + 1 <= g.leaf_size;
+                const bool rscan = rok && last - split <= g.leaf_size;
+                have_node = false;
+                if (lok && rok) {
+                    if (sp < STACK) sm.stack[sp++][tid] = rscan ? ((split + 1) | kScanFlag) : split + 1;
+                    else { atomicOr(g.err, kErrStack); q = -1; }
+                }
+                if (q >= 0) {
+                    if (lok) {
+                        if (lscan) { scan_k = max(first, lq + 1); scan_end = split; }
+                        else { node = split; have_node = true; }
+                    } else if (rok) {
+                        if (rscan) { scan_k = max(split + 1, lq + 1); scan_end = last; }
+                        else { node = split + 1; have_node = true; }
+                    }
+                }
+            }
+            if (q < 0) finished = sc;
+        }
+        scene_touch(g.done_ns, finished);
+        // 3. buffer the found pairs: < 32 held before the step, <= 64 added
+        unsigned incl = nf;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int tot = (int)__shfl_sync(kFull, incl, 31);
+        for (int j = 0; j < nf; ++j) sm.pairs[warp][npairs + (int)(incl - nf) + j] = f[j];
+        npairs += tot;
+        __syncwarp();
+        while (npairs >= 32) {
+            batch_process<DIM, CERT>(g, 32, sm.pairs[warp], sm.face[warp], sm.scene[warp], sm.code[warp]);
+            shift_pairs(sm.pairs[warp], 32, npairs);
+            npairs -= 32;
+        }
+    }
+    while (npairs > 0) {
+        const int m = npairs < 32 ? npairs : 32;
+        batch_process<DIM, CERT>(g, m, sm.pairs[warp], sm.face[warp], sm.scene[warp], sm.code[warp]);
+        shift_pairs(sm.pairs[warp], m, npairs);
+        npairs -= m;
+    }
+}
+
 // Per-scene results: counts 0, earliest-hit key (+inf, max).
 __global__ void k_b_init_results(unsigned long long *res, BestKey *best, int n)
 {
@@ -636,6 +925,8 @@ struct GroupHost {
     int4 *w_vf = nullptr, *w_ee = nullptr;
     Counters *w_cnt = nullptr;
     WaveState *ws = nullptr;
+    unsigned long long *queue = nullptr;   // persistent form's work queue
+    int fused_grid = 0;                    // persistent form's grid (resident blocks x SMs)
     cudaGraphConditionalHandle handle = 0;
 };
 
@@ -655,7 +946,9 @@ using namespace mclccd;
 struct mclccd_batch {
     int device = 0;
     int precision = MCLCCD_PREC_FP64;
-    int tune[4] = {128, 64, 16, 1};  // walk block size, walk stack, wave buffer (2^20 leaf pairs), leaf-scan size
+    // block size, stack depth, queue chunk, leaf-scan size, form (0 waves,
+    // 1 persistent), wave buffer (2^16 leaf pairs)
+    int tune[MCLCCD_BATCH_TUNE_COUNT] = {128, 64, 4, 1, MCLCCD_BATCH_FORM_WAVES, 512};
     int wave_chunk = 0;              // wave-buffer size the wave buffers were allocated for
     int n_scenes = 0;
     long long total_doubles = 0;
@@ -749,6 +1042,8 @@ BatchGroupDev group_view(mclccd_batch *b, GroupHost &G)
     g.n_hits = G.res; g.n_disc = G.res + 2 * G.n_scenes;
     g.n_sten = G.res + 3 * G.n_scenes; g.done_ns = G.res + 4 * G.n_scenes; g.best = G.best;
     g.rec = b->rec; g.n_rec = b->n_rec; g.rec_cap = b->rec_cap; g.err = &b->cnt->err;
+    g.queue = G.queue;
+    g.chunk = b->tune[MCLCCD_BATCH_TUNE_CHUNK];
     g.leaf_size = b->tune[MCLCCD_BATCH_TUNE_LEAF];
     return g;
 }
@@ -827,8 +1122,52 @@ void enqueue_wave(mclccd_batch *b, GroupHost &G, cudaStream_t st)
     k_wave_end<<<1, 1, 0, st>>>(G.ws, nq, G.cap_pairs, G.cap_vf, G.cap_ee, G.handle, &b->cnt->err);
 }
 
-// Whole step as a graph: build of each group, then its wave loop as a
-// conditional WHILE node whose body is one wave.
+// Persistent form.  prepare = true (outside capture): set the shared-memory
+// limit and compute the grid (every block resident); false: launch it.
+template <int DIM, bool CERT, int BLOCK, int STACK>
+cudaError_t fused_t(const BatchGroupDev &g, cudaStream_t st, bool prepare, int &grid)
+{
+    const size_t bytes = sizeof(FusedSmem<DIM, BLOCK, STACK>);
+    auto kern = k_batch_fused<DIM, CERT, BLOCK, STACK>;
+    if (prepare) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0, sms = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, bytes);
+        if (e != cudaSuccess) return e;
+        grid = std::max(1, per_sm) * std::max(1, sms);
+        return cudaSuccess;
+    }
+    kern<<<grid, BLOCK, bytes, st>>>(g);
+    return cudaGetLastError();
+}
+
+template <int DIM, bool CERT>
+cudaError_t fused_d(const BatchGroupDev &g, int block, int stack, cudaStream_t st, bool prepare, int &grid)
+{
+    if (block == 256)
+        return stack == 32 ? fused_t<DIM, CERT, 256, 32>(g, st, prepare, grid)
+                           : fused_t<DIM, CERT, 256, 64>(g, st, prepare, grid);
+    return stack == 32 ? fused_t<DIM, CERT, 128, 32>(g, st, prepare, grid)
+                       : fused_t<DIM, CERT, 128, 64>(g, st, prepare, grid);
+}
+
+cudaError_t fused(mclccd_batch *b, GroupHost &G, cudaStream_t st, bool prepare)
+{
+    const bool cert = b->precision == MCLCCD_PREC_FP32_CERTIFIED;
+    const int block = b->tune[MCLCCD_BATCH_TUNE_BLOCK], stack = b->tune[MCLCCD_BATCH_TUNE_STACK];
+    const BatchGroupDev g = group_view(b, G);
+    if (G.dim == 3)
+        return cert ? fused_d<3, true>(g, block, stack, st, prepare, G.fused_grid)
+                    : fused_d<3, false>(g, block, stack, st, prepare, G.fused_grid);
+    return cert ? fused_d<2, true>(g, block, stack, st, prepare, G.fused_grid)
+                : fused_d<2, false>(g, block, stack, st, prepare, G.fused_grid);
+}
+
+// Whole step as a graph: build of each group, then either its wave loop as
+// a conditional WHILE node whose body is one wave, or the persistent kernel.
 cudaError_t capture_step(mclccd_batch *b, cudaGraph_t *out)
 {
     cudaStream_t st = nullptr, body_st = nullptr;
@@ -846,6 +1185,11 @@ cudaError_t capture_step(mclccd_batch *b, cudaGraph_t *out)
         for (auto &G : b->grp) {
             if (G.np == 0 || e != cudaSuccess) continue;
             enqueue_build(b, G, st);
+            if (b->tune[MCLCCD_BATCH_TUNE_FORM] == MCLCCD_BATCH_FORM_PERSISTENT) {
+                cudaMemsetAsync(G.queue, 0, sizeof(unsigned long long), st);
+                e = fused(b, G, st, false);
+                continue;
+            }
             k_wave_init<<<1, 1, 0, st>>>(G.ws, 1ull << 16);
             cudaStreamCaptureStatus cs;
             cudaGraph_t graph = nullptr;
@@ -887,7 +1231,7 @@ cudaError_t capture_step(mclccd_batch *b, cudaGraph_t *out)
 // Wave buffers for the current wave-buffer tuning.
 cudaError_t ensure_wave_buffers(mclccd_batch *b)
 {
-    const int chunk = b->tune[MCLCCD_BATCH_TUNE_CHUNK];
+    const int chunk = b->tune[MCLCCD_BATCH_TUNE_WAVE];
     if (b->wave_chunk == chunk) return cudaSuccess;
     for (auto &G : b->grp) {
         for (void *p : {(void *)G.w_pairs, (void *)G.w_disc, (void *)G.w_vf, (void *)G.w_ee}) {
@@ -898,7 +1242,7 @@ cudaError_t ensure_wave_buffers(mclccd_batch *b)
         G.w_pairs = G.w_disc = nullptr;
         G.w_vf = G.w_ee = nullptr;
         if (G.np == 0) continue;
-        G.cap_pairs = (unsigned long long)chunk << 20;
+        G.cap_pairs = (unsigned long long)chunk << 16;
         G.cap_vf = 2 * G.cap_pairs;
         G.cap_ee = G.dim == 3 ? 4 * G.cap_pairs : 0;
         G.cap_disc = G.cap_pairs;
@@ -1056,6 +1400,7 @@ int mclccd_batch_set_scenes(mclccd_batch *b, int n_scenes, const int *scene_dim,
         MB_CUDA(b, balloc(b, G.vert_scene, std::max<size_t>(nv, 1)));
         MB_CUDA(b, balloc(b, G.w_cnt, 1));
         MB_CUDA(b, balloc(b, G.ws, 1));
+        MB_CUDA(b, balloc(b, G.queue, 1));
         MB_CUDA(b, cudaMemsetAsync(G.ws, 0, sizeof(WaveState), st));
         MB_CUDA(b, balloc(b, G.dst_off, G.n_scenes + 1));
         MB_CUDA(b, balloc(b, G.src_off, G.n_scenes));
@@ -1143,7 +1488,10 @@ int mclccd_batch_set_tuning(mclccd_batch *b, int key, int value)
     const bool ok = (key == MCLCCD_BATCH_TUNE_BLOCK && (value == 128 || value == 256)) ||
                     (key == MCLCCD_BATCH_TUNE_STACK && (value == 32 || value == 64)) ||
                     (key == MCLCCD_BATCH_TUNE_CHUNK && value >= 1 && value <= 64) ||
-                    (key == MCLCCD_BATCH_TUNE_LEAF && value >= 1 && value <= 16);
+                    (key == MCLCCD_BATCH_TUNE_LEAF && value >= 1 && value <= 16) ||
+                    (key == MCLCCD_BATCH_TUNE_FORM &&
+                     (value == MCLCCD_BATCH_FORM_WAVES || value == MCLCCD_BATCH_FORM_PERSISTENT)) ||
+                    (key == MCLCCD_BATCH_TUNE_WAVE && value >= 1 && value <= 1024);
     if (!ok) return MCLCCD_ERR_INVALID;
     if (b->tune[key] != value) b->dirty = true;
     b->tune[key] = value;
@@ -1154,6 +1502,23 @@ int mclccd_batch_get_tuning(const mclccd_batch *b, int key, int *value)
 {
     if (!b || !value || key < 0 || key >= MCLCCD_BATCH_TUNE_COUNT) return MCLCCD_ERR_INVALID;
     *value = b->tune[key];
+    return MCLCCD_OK;
+}
+
+int mclccd_batch_wave_stats(mclccd_batch *b, long long *waves, long long *redos)
+{
+    if (!b || !waves || !redos) return MCLCCD_ERR_INVALID;
+    *waves = *redos = 0;
+    if (!b->ran || b->tune[MCLCCD_BATCH_TUNE_FORM] != MCLCCD_BATCH_FORM_WAVES) return MCLCCD_OK;
+    cudaSetDevice(b->device);
+    for (auto &G : b->grp) {
+        if (G.np == 0 || !G.ws) continue;
+        WaveState h{};
+        MB_CUDA(b, cudaMemcpyAsync(&h, G.ws, sizeof(h), cudaMemcpyDeviceToHost, b->stream));
+        MB_CUDA(b, cudaStreamSynchronize(b->stream));
+        *waves += (long long)h.waves;
+        *redos += (long long)h.redos;
+    }
     return MCLCCD_OK;
 }
 
@@ -1172,9 +1537,13 @@ int mclccd_batch_run(mclccd_batch *b, void *stream)
     }
     if (b->dirty) {
         MB_CUDA(b, cudaStreamSynchronize(st));
-        MB_CUDA(b, ensure_wave_buffers(b));
-        for (auto &G : b->grp)
-            if (G.np > 0) MB_CUDA(b, prepare_walk(G.dim, b->tune[MCLCCD_BATCH_TUNE_BLOCK], b->tune[MCLCCD_BATCH_TUNE_STACK]));
+        const bool persistent = b->tune[MCLCCD_BATCH_TUNE_FORM] == MCLCCD_BATCH_FORM_PERSISTENT;
+        if (!persistent) MB_CUDA(b, ensure_wave_buffers(b));
+        for (auto &G : b->grp) {
+            if (G.np == 0) continue;
+            if (persistent) MB_CUDA(b, fused(b, G, st, true));
+            else MB_CUDA(b, prepare_walk(G.dim, b->tune[MCLCCD_BATCH_TUNE_BLOCK], b->tune[MCLCCD_BATCH_TUNE_STACK]));
+        }
         if (b->exec) cudaGraphExecDestroy(b->exec);
         if (b->graph) cudaGraphDestroy(b->graph);
         b->exec = nullptr;

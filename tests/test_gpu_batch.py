@@ -7,7 +7,7 @@ import pytest
 
 from mclccd_b200 import PREC_FP32_CERTIFIED, PREC_FP64, BVHTree, scenes
 from mclccd_b200.autotune import tune_batch
-from mclccd_b200.batch import Batch
+from mclccd_b200.batch import FORM_PERSISTENT, FORM_WAVES, Batch
 
 pytestmark = pytest.mark.gpu
 
@@ -70,13 +70,35 @@ def test_batch_every_tuning_same_results():
     exp = [expected(s) for s in sc]
     b = Batch()
     b.set_scenes(sc)
-    for block in (128, 256):
-        for stack in (32, 64):
-            for chunk in (1, 7):
-                for leaf in (1, 4):
-                    b.set_tuning(block=block, stack=stack, chunk=chunk, leaf=leaf)
-                    b.run()
-                    check(b.results(), exp)
+    for form in (FORM_WAVES, FORM_PERSISTENT):
+        for block in (128, 256):
+            for stack in (32, 64):
+                for knob in (1, 7):   # wave buffer (waves) or queue chunk (persistent)
+                    for leaf in (1, 4):
+                        b.set_tuning(form=form, block=block, stack=stack, leaf=leaf,
+                                     **({"wave": knob} if form == FORM_WAVES else {"chunk": knob}))
+                        b.run()
+                        check(b.results(), exp)
+
+
+def test_batch_waves_redo_on_overflow():
+    # a 128 x 128 fold has far more leaf pairs than a 2^16-pair wave buffer
+    # holds: the first waves overflow and are redone with fewer queries
+    sc = [scenes.folded_cloth(128, seed=11), scenes.annulus_2d(700, seed=12), scenes.folded_cloth(20, seed=13)]
+    exp = [expected(s) for s in sc]
+    b = Batch()
+    b.set_scenes(sc)
+    b.set_tuning(form=FORM_WAVES, wave=1)
+    b.run()
+    check(b.results(), exp)
+    waves, redos = b.wave_stats()
+    assert redos > 0 and waves > 2, (waves, redos)
+    b.run()   # the adapted wave size carries over: same results
+    check(b.results(), exp)
+    b.set_tuning(form=FORM_PERSISTENT)
+    b.run()
+    check(b.results(), exp)
+    assert b.wave_stats() == (0, 0)
 
 
 def test_batch_certified():
@@ -84,12 +106,14 @@ def test_batch_certified():
     exp = [expected(s) for s in sc]
     b = Batch(precision=PREC_FP32_CERTIFIED)
     b.set_scenes(sc)
-    b.run()
-    r = b.results()
-    check(r, exp, exact=False)
-    for s, e in enumerate(exp):
-        if e["n_hits"]:
-            assert r["min_toi"][s] <= e["min_toi"] and r["min_toi"][s] >= e["min_toi"] * (1 - 1e-6)
+    for form in (FORM_WAVES, FORM_PERSISTENT):
+        b.set_tuning(form=form)
+        b.run()
+        r = b.results()
+        check(r, exp, exact=False)
+        for s, e in enumerate(exp):
+            if e["n_hits"]:
+                assert r["min_toi"][s] <= e["min_toi"] and r["min_toi"][s] >= e["min_toi"] * (1 - 1e-6)
 
 
 def test_batch_new_positions_and_autotune():
@@ -99,7 +123,9 @@ def test_batch_new_positions_and_autotune():
     rng = np.random.default_rng(4)
     V1s = [s[1] + rng.normal(0, 1e-3, s[1].shape) for s in sc]
     b.set_positions([s[0] for s in sc], V1s)
-    best, table = tune_batch(b, space={"block": (128,), "stack": (64,), "chunk": (1, 4), "leaf": (1, 2)}, repeats=1)
+    best, table = tune_batch(b, space={"form": (0, 1), "block": (128,), "stack": (64,), "chunk": (1, 4), "leaf": (1, 2),
+                                       "wave": (1, 512)}, repeats=1)
+    assert len(table) == 8   # each form varies only its own knob
     assert best in [c for c, t in table if t is not None]
     b.run()
     check(b.results(), [expected((s[0], v1, s[2], s[3])) for s, v1 in zip(sc, V1s)])
