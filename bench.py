@@ -504,7 +504,7 @@ def measure_batch(args):
     tb = Batch()
     tb.set_scenes(sample)
     best, table = tune_batch(tb, space={"form": (0, 1), "block": (128, 256), "stack": (64,), "chunk": (1, 4),
-                                        "leaf": (1, 2), "wave": (512, 1024)}, repeats=1)
+                                        "leaf": (1, 2), "wave": (2048, 4096)}, repeats=1)
     del tb, sample
     full = [s for _, s in scenes.batch_scenes()]
     tris = int(sum(len(s[2]) for s in full))

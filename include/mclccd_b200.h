@@ -228,7 +228,7 @@ typedef struct mclccd_batch mclccd_batch;
 #define MCLCCD_BATCH_TUNE_CHUNK 2   /* persistent form: queries per lane a warp takes from the work queue: 1..64 */
 #define MCLCCD_BATCH_TUNE_LEAF 3    /* subtrees of up to this many leaves are scanned, not descended: 1..16 */
 #define MCLCCD_BATCH_TUNE_FORM 4    /* MCLCCD_BATCH_FORM_WAVES (default) or MCLCCD_BATCH_FORM_PERSISTENT */
-#define MCLCCD_BATCH_TUNE_WAVE 5    /* waves form: wave buffer, in 2^16 leaf pairs (stencil buffers 2x VF, 4x EE): 1..1024 */
+#define MCLCCD_BATCH_TUNE_WAVE 5    /* waves form: wave buffer, in 2^16 leaf pairs (stencil buffers 2x VF, 4x EE): 1..4096 */
 #define MCLCCD_BATCH_TUNE_COUNT 6
 /* Forms of the batched step.  WAVES: per group, a device-driven loop of
  * waves (walk -> stencil expansion -> ACCD -> per-scene reductions) in a
@@ -285,12 +285,17 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
 
 /* No counterpart in the reference: launch-shape knobs of the device path
  * (chosen by the autotuner, mclccd_b200/autotune.py).  Keys: grid size (in
- * blocks) of the stencil-expansion kernel and of the ACCD kernels, and the
- * tree-walk form (1: warp-cooperative packets, 0: one query per thread). */
+ * blocks) of the stencil-expansion kernel and of the ACCD kernels, the
+ * tree-walk form (1: warp-cooperative packets, 0: one query per thread) and
+ * the FP64 ACCD form (1: stencils that go on after the first distance are
+ * re-binned in shared memory so warps run heads or tails, never both; 0, the
+ * default and faster on B200: one stencil per thread start to end).  Results
+ * do not depend on any of them. */
 #define MCLCCD_TUNE_EXPAND_GRID 0
 #define MCLCCD_TUNE_ACCD_GRID 1
 #define MCLCCD_TUNE_WALK_PACKET 2
-#define MCLCCD_TUNE_COUNT 3
+#define MCLCCD_TUNE_ACCD_REBIN 3
+#define MCLCCD_TUNE_COUNT 4
 int mclccd_set_tuning(mclccd_tree *tree, int key, int value);
 int mclccd_get_tuning(const mclccd_tree *tree, int key, int *value);
 

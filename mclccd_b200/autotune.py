@@ -21,7 +21,7 @@ import numpy as np
 from .ccd import CCDError
 
 DEFAULT_SPACE = {"form": (0, 1), "block": (128, 256), "stack": (32, 64), "chunk": (1, 4, 16), "leaf": (1, 4),
-                 "wave": (256, 512, 1024)}
+                 "wave": (1024, 2048, 4096)}
 # knobs that only one form reads
 _UNUSED = {0: ("chunk",), 1: ("wave",)}
 

@@ -410,24 +410,35 @@ __global__ void k_wave_check_sten(WaveState *ws, Counters *wc, unsigned long lon
     }
 }
 
-// Advances the loop: a voided wave is redone with half the queries; a
-// done wave moves the cursor and may double the next wave.  Sets the loop
-// condition.  A single query that cannot fit, or a runaway loop, stops it
-// with an error.
+// Advances the loop and sizes the next wave from this one's demand: the
+// fullest buffer (pairs, VF or EE stencils; the counters keep counting past
+// capacity) should come to about 60% full: pair density grows along the
+// small-first scene order, and a redo costs a wasted walk.  A voided wave is
+// redone with at most half its queries; a done wave moves the cursor and may
+// grow the next one up to 2x.  Sets the loop condition.  A single query that cannot fit,
+// or a runaway loop, stops it with an error.
 __global__ void k_wave_end(WaveState *ws, unsigned long long n_total, unsigned long long cap_pairs,
                            unsigned long long cap_vf, unsigned long long cap_ee, cudaGraphConditionalHandle handle,
                            unsigned *err)
 {
+    const unsigned long long nq = ws->q1 - ws->q0;
+    double fill = (double)ws->used_pairs / (double)cap_pairs;
+    fill = fmax(fill, (double)ws->used_vf / (double)cap_vf);
+    if (cap_ee) fill = fmax(fill, (double)ws->used_ee / (double)cap_ee);
     if (ws->redo) {
         ++ws->redos;
-        if (ws->wave_q <= 1) { atomicOr(err, kErrWave); ws->stop = 1; }
-        else ws->wave_q >>= 1;
+        if (nq <= 1) { atomicOr(err, kErrWave); ws->stop = 1; }
+        else {
+            double q = fill > 1.0 ? (double)nq * (0.6 / fill) : 0.5 * (double)nq;
+            q = fmin(q, 0.5 * (double)nq);
+            ws->wave_q = q < 1.0 ? 1ull : (unsigned long long)q;
+        }
     } else {
         ws->cursor = ws->q1;
         ++ws->waves;
-        if (4 * ws->used_pairs < cap_pairs && 4 * ws->used_vf < cap_vf && 4 * ws->used_ee < cap_ee &&
-            ws->wave_q < n_total)
-            ws->wave_q <<= 1;
+        const double grow = fill > 0.3 ? 0.6 / fill : 2.0;
+        const double q = (double)nq * grow;
+        ws->wave_q = q < 1.0 ? 1ull : q > (double)n_total ? n_total : (unsigned long long)q;
     }
     if (ws->waves + ws->redos > (1ull << 24)) { atomicOr(err, kErrWave); ws->stop = 1; }
     cudaGraphSetConditional(handle, (!ws->stop && ws->cursor < n_total) ? 1u : 0u);
@@ -948,7 +959,7 @@ struct mclccd_batch {
     int precision = MCLCCD_PREC_FP64;
     // block size, stack depth, queue chunk, leaf-scan size, form (0 waves,
     // 1 persistent), wave buffer (2^16 leaf pairs)
-    int tune[MCLCCD_BATCH_TUNE_COUNT] = {128, 64, 4, 1, MCLCCD_BATCH_FORM_WAVES, 512};
+    int tune[MCLCCD_BATCH_TUNE_COUNT] = {128, 64, 4, 1, MCLCCD_BATCH_FORM_WAVES, 2048};
     int wave_chunk = 0;              // wave-buffer size the wave buffers were allocated for
     int n_scenes = 0;
     long long total_doubles = 0;
@@ -1491,7 +1502,7 @@ int mclccd_batch_set_tuning(mclccd_batch *b, int key, int value)
                     (key == MCLCCD_BATCH_TUNE_LEAF && value >= 1 && value <= 16) ||
                     (key == MCLCCD_BATCH_TUNE_FORM &&
                      (value == MCLCCD_BATCH_FORM_WAVES || value == MCLCCD_BATCH_FORM_PERSISTENT)) ||
-                    (key == MCLCCD_BATCH_TUNE_WAVE && value >= 1 && value <= 1024);
+                    (key == MCLCCD_BATCH_TUNE_WAVE && value >= 1 && value <= 4096);
     if (!ok) return MCLCCD_ERR_INVALID;
     if (b->tune[key] != value) b->dirty = true;
     b->tune[key] = value;

@@ -68,7 +68,7 @@ struct mclccd_tree {
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
     cudaEvent_t ev[8] = {};
-    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0};
+    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0};
 };
 
 namespace {
@@ -452,7 +452,7 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
                 } else {
                     launch_accd_pipeline(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
                                          as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
-                                         t->tune[MCLCCD_TUNE_ACCD_GRID], st);
+                                         t->tune[MCLCCD_TUNE_ACCD_GRID], t->tune[MCLCCD_TUNE_ACCD_REBIN] != 0, st);
                     ++t->launches;
                 }
             };
@@ -829,7 +829,8 @@ int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)
 int mclccd_set_tuning(mclccd_tree *t, int key, int value)
 {
     if (!t || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
-    if (key == MCLCCD_TUNE_WALK_PACKET ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))
+    const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_ACCD_REBIN;
+    if (flag ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))
         return fail(t, MCLCCD_ERR_INVALID, "tuning value out of range");
     t->tune[key] = value;
     return MCLCCD_OK;

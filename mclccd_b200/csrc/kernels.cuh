@@ -35,7 +35,8 @@ void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap
 // narrow.cu
 void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
-                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st);
+                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, bool rebin,
+                          cudaStream_t st);
 // certified.cu
 void launch_accd_certified(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr,
                            unsigned long long cap, const double *V0, const double *V1, int nv, double eta,

@@ -69,6 +69,122 @@ k_accd_pipeline(const int4 *__restrict__ sten, const unsigned long long *n_ptr, 
     }
 }
 
+// Re-binned pipeline form: the head of ACCD (setup, first distance,
+// immediate hit, the miss decided before iteration 1's distance) runs for
+// one stencil per thread; stencils that go on are queued in shared memory
+// with their first distance d0 and motion bound l_p, and whenever a full
+// block's worth is queued every thread runs the tail of one of them.  A
+// warp then runs either heads or tails, never both, so the lanes that miss
+// after one distance no longer idle through the others' two or more.  The
+// tail rebuilds the exact state entering iteration 1 -- x = v0, toi = 0,
+// t_l and g from d0 and l_p, p from a re-gather (setup without the norms)
+// -- so (hit, toi) are bit-identical to the unbinned kernel.  A stencil
+// whose iteration 0 is not an exact no-op runs its tail in place (rare).
+constexpr int kRebinBlock = 128;
+
+template <int DIM, bool VF>
+__device__ __forceinline__ void rebin_emit(const int4 &s4, double toi, bool ok, Counters *cnt, int4 *hit_sten,
+                                           double *hit_toi, unsigned char *hit_isvf, unsigned long long hit_cap)
+{
+    if (ok) {
+        const unsigned long long slot = warp_append(&cnt->n_hits);
+        if (slot < hit_cap) {
+            hit_sten[slot] = s4;
+            hit_toi[slot] = toi;
+            hit_isvf[slot] = VF ? 1 : 0;
+        }
+    }
+}
+
+template <int DIM, bool VF>
+__global__ void __launch_bounds__(kRebinBlock, MCLCCD_ACCD_MIN_BLOCKS)
+k_accd_rebin(const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
+             const double *__restrict__ V0, const double *__restrict__ V1, int nv, double eta,
+             int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,
+             unsigned long long hit_cap, Counters *cnt)
+{
+    __shared__ int4 q_sten[2 * kRebinBlock];
+    __shared__ double q_d0[2 * kRebinBlock], q_lp[2 * kRebinBlock];
+    __shared__ int q_n;
+    unsigned long long n = *(volatile const unsigned long long *)n_ptr;
+    if (n > cap) n = cap;
+    const int tid = threadIdx.x;
+    if (tid == 0) q_n = 0;
+    __syncthreads();
+    const double xx = eta * eta;
+    auto tail = [&](int j) {   // tail of queued stencil j
+        const int4 s4 = q_sten[j];
+        const double d0 = q_d0[j], l_p = q_lp[j];
+        const int s[4] = {s4.x, s4.y, s4.z, s4.w};
+        double v0[DIM + 1][DIM], v1[DIM + 1][DIM], p[DIM + 1][DIM], x[DIM + 1][DIM], unused;
+        bool noop;
+        gather_stencil<DIM>(s, V0, V1, nv, v0, v1);   // indices checked by the head
+        accd_setup<DIM, VF, false>(v0, v1, p, x, unused, noop);
+        const double A = d0 * d0 - xx;
+        const double g = (1.0 * A) / (d0 - eta);
+        double toi = 0.0;
+        int iters;
+        const int hit = accd_tail<DIM, VF>(x, p, l_p, eta, g, toi, 0.9 * A / ((d0 + eta) * l_p), iters);
+        if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
+        return hit && toi >= 0.0 ? toi : -1.0;
+    };
+    const unsigned long long stride = (unsigned long long)gridDim.x * kRebinBlock;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * kRebinBlock; base < n; base += stride) {
+        const unsigned long long i = base + tid;
+        int4 s4 = make_int4(0, 0, 0, 0);
+        double toi = -1.0;
+        bool hit = false;
+        if (i < n) {
+            s4 = sten[i];
+            const int s[4] = {s4.x, s4.y, s4.z, s4.w};
+            double v0[DIM + 1][DIM], v1[DIM + 1][DIM];
+            if (!gather_stencil<DIM>(s, V0, V1, nv, v0, v1)) {
+                atomicOr(&cnt->err, kErrBadIndex);
+            } else {
+                double p[DIM + 1][DIM], x[DIM + 1][DIM], l_p, d0, g, t_l;
+                bool noop, skip;
+                accd_setup<DIM, VF, true>(v0, v1, p, x, l_p, noop);
+                const int h = accd_head<DIM, VF>(x, p, l_p, noop, eta, d0, g, toi, t_l, skip);
+                if (h == kHeadHit) {
+                    hit = toi >= 0.0;
+                } else if (h == kHeadContinue) {
+                    if (skip) {
+                        const int j = atomicAdd(&q_n, 1);   // < 2 * kRebinBlock: < kRebinBlock held before
+                        q_sten[j] = s4;
+                        q_d0[j] = d0;
+                        q_lp[j] = l_p;
+                    } else {
+                        int iters;
+                        hit = accd_tail<DIM, VF>(x, p, l_p, eta, g, toi, t_l, iters) && toi >= 0.0;
+                        if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
+                    }
+                }
+            }
+        }
+        rebin_emit<DIM, VF>(s4, toi, hit, cnt, hit_sten, hit_toi, hit_isvf, hit_cap);
+        __syncthreads();
+        const int queued = q_n;
+        if (queued >= kRebinBlock) {   // one tail per thread
+            const double t = tail(tid);
+            rebin_emit<DIM, VF>(q_sten[tid], t, t >= 0.0, cnt, hit_sten, hit_toi, hit_isvf, hit_cap);
+            __syncthreads();
+            const int left = queued - kRebinBlock;
+            int4 ms;
+            double md = 0, ml = 0;
+            if (tid < left) { ms = q_sten[kRebinBlock + tid]; md = q_d0[kRebinBlock + tid]; ml = q_lp[kRebinBlock + tid]; }
+            __syncthreads();
+            if (tid < left) { q_sten[tid] = ms; q_d0[tid] = md; q_lp[tid] = ml; }
+            if (tid == 0) q_n = left;
+            __syncthreads();
+        }
+    }
+    const int queued = q_n;   // last partial bin
+    if (tid < queued) {
+        const double t = tail(tid);
+        rebin_emit<DIM, VF>(q_sten[tid], t, t >= 0.0, cnt, hit_sten, hit_toi, hit_isvf, hit_cap);
+    }
+}
+
 // Bulk form: caller-given stencils (int32 x 4 each, any alignment), per-stencil
 // outputs in input order.  toi = -1 on a miss, as default_narrow_phase returns.
 template <int DIM>
@@ -98,8 +214,18 @@ k_accd_bulk(const int *__restrict__ sten, const unsigned char *__restrict__ is_v
 
 void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
-                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st)
+                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, bool rebin,
+                          cudaStream_t st)
 {
+    if (rebin) {
+        if (dim == 3) {
+            if (vf) k_accd_rebin<3, true><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+            else k_accd_rebin<3, false><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+        } else {
+            k_accd_rebin<2, true><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+        }
+        return;
+    }
     if (dim == 3) {
         if (vf) k_accd_pipeline<3, true><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
         else k_accd_pipeline<3, false><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);

@@ -87,6 +87,20 @@ def test_cfg0_folded_cloth(port):
     check_against_port(t, port, V0, V1, F, eta)
 
 
+@pytest.mark.parametrize("dim", [3, 2])
+def test_rebinned_accd_against_port(port, dim):
+    # the re-binned ACCD form (heads and tails in separate warp passes) gives
+    # the same bits as the default one-stencil-per-thread form
+    V0, V1, F, eta = scenes.folded_cloth(48, seed=21) if dim == 3 else scenes.annulus_2d(300, seed=22)
+    t = BVHTree(dim)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.set_tuning(accd_rebin=1)
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    assert t.get_tuning()["accd_rebin"] == 1
+    check_against_port(t, port, V0, V1, F, eta)
+
+
 @pytest.mark.parametrize("scene", ["wavy129", "spheres", "annulus", "fold_big_motion"])
 def test_scenes_against_port(port, scene):
     V0, V1, F, eta = {
