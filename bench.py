@@ -50,6 +50,10 @@ def parse(argv=None):
     ap.add_argument("--no-forms", action="store_true", help="skip the certified/adjoint/batch form measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-scene batch measurement")
     ap.add_argument("--tune", default="", help="launch knobs, e.g. walk_packet=0,accd_grid=2368")
+    ap.add_argument("--batch-only", action="store_true", help="only the batching form (prints its JSON object)")
+    ap.add_argument("--batch-scenes", default="384,128", help="batching form: 3D cloths,2D annuli")
+    ap.add_argument("--batch-tune", default="", help="batching form: fixed knobs instead of the autotuner, "
+                                                     "e.g. form=0,wave=4096")
     return ap.parse_args(argv)
 
 
@@ -248,6 +252,10 @@ def run_b200(args, rank, world, local):
     import torch
     from mclccd_b200 import MEM_HOST, PREC_FP32_CERTIFIED, PREC_FP64, BVHTree, scenes
     torch.cuda.set_device(local)
+    if args.batch_only:
+        if rank == 0:
+            print(json.dumps(measure_batch(args)), flush=True)
+        return 0
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -495,37 +503,53 @@ def measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev):
 def measure_batch(args):
     """Batching form: 512 scenes (384 folded cloths, side log-uniform in
     [16, 384]; 128 2D annuli, ring resolution U[32, 2048]) per run, one CUDA
-    graph.  The autotuner picks the launch knobs on a 64-scene sample; the
-    full batch then runs once to capture and warm up, once timed."""
-    from mclccd_b200 import scenes
+    graph.  The autotuner picks the form and launch knobs on a 64-scene
+    sample (or --batch-tune fixes them); the full batch then runs once to
+    capture and warm up and once timed, in FP64 and in the FP32-certified
+    form."""
+    from mclccd_b200 import PREC_FP32_CERTIFIED, PREC_FP64, scenes
     from mclccd_b200.autotune import tune_batch
     from mclccd_b200.batch import Batch
-    sample = [s for _, s in scenes.batch_scenes(n3d=48, n2d=16, seed=1)]
-    tb = Batch()
-    tb.set_scenes(sample)
-    best, table = tune_batch(tb, space={"form": (0, 1), "block": (128, 256), "stack": (64,), "chunk": (1, 4),
-                                        "leaf": (1, 2), "wave": (2048, 4096)}, repeats=1)
-    del tb, sample
-    full = [s for _, s in scenes.batch_scenes()]
+    n3d, n2d = (int(x) for x in args.batch_scenes.split(","))
+    if args.batch_tune:
+        best, table = {k: int(v) for k, v in (kv.split("=") for kv in args.batch_tune.split(","))}, []
+    else:
+        sample = [s for _, s in scenes.batch_scenes(n3d=48, n2d=16, seed=1)]
+        tb = Batch()
+        tb.set_scenes(sample)
+        best, table = tune_batch(tb, space={"form": (0, 1), "block": (128, 256), "stack": (64,), "chunk": (1, 4),
+                                            "leaf": (1, 2), "wave": (2048, 4096)}, repeats=1)
+        del tb, sample
+    full = [s for _, s in scenes.batch_scenes(n3d=n3d, n2d=n2d)]
+    ns = len(full)
     tris = int(sum(len(s[2]) for s in full))
     b = Batch()
     b.set_scenes(full)
     b.set_tuning(**best)
-    b.run()
-    b.results()
-    b.run()
-    r = b.results()
-    ms = r["batch_ms"]
-    d = r["done_ms"]
-    nst = int(r["n_stencils"].sum())
-    return {"workload": "512 scenes: 384 folded cloths (side log-uniform [16, 384], thickness 1e-3) + 128 2D "
-                        "annuli (ring U[32, 2048]), FP64, one CUDA graph per run",
-            "tris": tris, "batch_ms": ms, "scenes_per_s": 512 / ms * 1e3, "stencils": nst,
-            "stencils_per_s": nst / ms * 1e3, "hits": int(r["n_hits"].sum()),
-            "scene_latency_ms": {"p50": float(np.percentile(d, 50)), "p99": float(np.percentile(d, 99)),
-                                 "max": float(d.max())},
-            "tuning": best, "tuning_table": [[c, t] for c, t in table]}
-
+    runs = {}
+    for name, prec in (("fp64", PREC_FP64), ("fp32cert", PREC_FP32_CERTIFIED)):
+        b.set_precision(prec)
+        b.run()
+        b.results()
+        b.run()
+        r = b.results()
+        ms, d = r["batch_ms"], r["done_ms"]
+        nst = int(r["n_stencils"].sum())
+        runs[name] = {"batch_ms": ms, "scenes_per_s": ns / ms * 1e3, "stencils": nst,
+                      "stencils_per_s": nst / ms * 1e3, "hits": int(r["n_hits"].sum()),
+                      "waves_redos": list(b.wave_stats()),
+                      "scene_latency_ms": {"p50": float(np.percentile(d, 50)), "p99": float(np.percentile(d, 99)),
+                                           "max": float(d.max())}}
+        if name == "fp64":
+            ref = r
+        else:
+            runs[name]["same_hit_counts_as_fp64"] = bool(np.array_equal(r["n_hits"], ref["n_hits"]))
+    out = {"workload": f"{ns} scenes: {n3d} folded cloths (side log-uniform [16, 384], thickness 1e-3) + {n2d} 2D "
+                       "annuli (ring U[32, 2048]), one CUDA graph per run",
+           "tris": tris, "tuning": best, "tuning_table": [[c, t] for c, t in table]}
+    out.update(runs["fp64"])
+    out["fp32cert"] = runs["fp32cert"]
+    return out
 
 def main():
     args = parse()
