@@ -38,7 +38,7 @@ typedef struct mclccd_tree mclccd_tree;
 #define MCLCCD_ERR_OVERFLOW 4    /* caller's output capacity too small (copied a prefix) */
 #define MCLCCD_ERR_STATE 5       /* traverse before update, or results before traverse */
 #define MCLCCD_ERR_DEVICE 6      /* a kernel gave up a bounded wait or overflowed its stack */
-#define MCLCCD_ERR_UNSUPPORTED 7 /* option not provided by this path (vf_one_sided) */
+#define MCLCCD_ERR_UNSUPPORTED 7 /* option combination not provided (bulk: one-sided VF with the certified form) */
 #define MCLCCD_ERR_SCRATCH_LIMIT 8 /* mclccd_narrow_phase_bulk_static: arrays exceed its fixed scratch */
 
 /* Where caller arrays live. */
@@ -50,7 +50,7 @@ typedef struct mclccd_tree mclccd_tree;
 #define MCLCCD_OPT_THREADED (1u << 1)     /* accepted; the device path is always parallel */
 #define MCLCCD_OPT_DISCRETE (1u << 2)
 #define MCLCCD_OPT_CONTINUOUS (1u << 3)
-#define MCLCCD_OPT_VF_ONE_SIDED (1u << 4) /* CTCD narrow phase: not provided (UNSUPPORTED) */
+#define MCLCCD_OPT_VF_ONE_SIDED (1u << 4) /* VF narrow phase: CTCD with the wrong-side test (NarrowPhase.cpp:338-425) */
 #define MCLCCD_OPT_EE_ROBUST (1u << 5)    /* accepted; unused by ACCD, as in the reference */
 #define MCLCCD_OPT_DEFAULT (MCLCCD_OPT_REPTRI | MCLCCD_OPT_THREADED | MCLCCD_OPT_DISCRETE | \
                             MCLCCD_OPT_CONTINUOUS | MCLCCD_OPT_EE_ROBUST)
@@ -135,7 +135,13 @@ int mclccd_narrow_phase_bulk(int dim, const double *V0, const double *V1, int nv
 /* The bulk narrow phase with a precision: MCLCCD_PREC_FP64 (same as above) or
  * MCLCCD_PREC_FP32_CERTIFIED (identical hit/miss; toi never later than the
  * FP64 value and within 1e-6 relative of it).  n_fp64 (may be NULL) receives
- * how many stencils the certified form had to evaluate in full FP64. */
+ * how many stencils the certified form had to evaluate in full FP64.
+ * MCLCCD_PREC_FP64 | MCLCCD_BULK_VF_ONE_SIDED: VF stencils take the one-sided
+ * CTCD narrow phase instead (NarrowPhaseCTCD::query_ccd_vf with the
+ * wrong-side test, as BVHTree with vf_one_sided); a hit is a contact on the
+ * right side, wrong-side-only contacts are misses.  With the certified form
+ * it returns MCLCCD_ERR_UNSUPPORTED. */
+#define MCLCCD_BULK_VF_ONE_SIDED 0x100
 int mclccd_narrow_phase_bulk_ex(int dim, const double *V0, const double *V1, int nv, const int *sten,
                                 const unsigned char *is_vf, long long n, double vf_ccd_eta, double ee_ccd_eta,
                                 double *out_toi, int *out_hit, int mem_kind, void *stream, int precision,

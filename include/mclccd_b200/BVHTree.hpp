@@ -61,7 +61,7 @@ public:
         bool threaded = true;      // accepted; the GPU path is always parallel
         bool discrete = true;      // discrete check ff/ee at V1
         bool continuous = true;    // ccd check from V0 to V1
-        bool vf_one_sided = false; // CTCD narrow phase: not provided (throws)
+        bool vf_one_sided = false; // VF narrow phase: CTCD with the wrong-side test
         bool ee_robust = true;     // unused by ACCD, as in the reference
     } options;
 

@@ -31,6 +31,7 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_OVERFLOW, ERR_STATE, ERR_DEVICE, ERR_U
 MEM_HOST, MEM_DEVICE = 0, 1
 OPT_REPTRI, OPT_THREADED, OPT_DISCRETE, OPT_CONTINUOUS = 1, 2, 4, 8
 OPT_VF_ONE_SIDED, OPT_EE_ROBUST = 16, 32
+BULK_VF_ONE_SIDED = 0x100
 OPT_ALWAYS_REBUILD, OPT_PROFILE = 1 << 8, 1 << 9
 PREC_FP64, PREC_FP32_CERTIFIED = 0, 1
 
@@ -347,13 +348,17 @@ class BVHTree:
 
 
 def narrow_phase_bulk(V0, V1, sten, is_vf, vf_eta, ee_eta=None, stream: int | None = None,
-                      precision: int = PREC_FP64, return_fallbacks: bool = False):
+                      precision: int = PREC_FP64, return_fallbacks: bool = False, vf_one_sided: bool = False):
     """NarrowPhaseACCD::query_ccd_vf/ee over a stencil array on the GPU.
     Returns (toi, hit); toi is -1 where hit == 0.  With
     precision=PREC_FP32_CERTIFIED and return_fallbacks, also the number of
-    stencils that needed full FP64."""
+    stencils that needed full FP64.  vf_one_sided: VF stencils take the
+    one-sided CTCD narrow phase (NarrowPhaseCTCD::query_ccd_vf with the
+    wrong-side test), as BVHTree does with options.vf_one_sided."""
     L = lib()
     ee_eta = vf_eta if ee_eta is None else ee_eta
+    if vf_one_sided:
+        precision |= BULK_VF_ONE_SIDED
     nfb = C.c_longlong()
     if _is_torch_cuda(V0):
         import torch

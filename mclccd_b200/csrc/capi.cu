@@ -230,8 +230,6 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
     t->err.clear();
     if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
     if (np < 0 || nv < 0) return fail(t, MCLCCD_ERR_INVALID, "negative size");
-    if (t->flags & MCLCCD_OPT_VF_ONE_SIDED)
-        return fail(t, MCLCCD_ERR_UNSUPPORTED, "vf_one_sided (CTCD narrow phase) is not provided");
     if (!(t->box_eta >= 0) || !(t->vf_eta >= 0) || !(t->ee_eta >= 0)) return fail(t, MCLCCD_ERR_INVALID, "etas must be >= 0");
     // BVHTree.cpp:39-40: the narrow-phase gaps never exceed the box padding.
     t->vf_eta = std::min(t->vf_eta, t->box_eta);
@@ -364,8 +362,6 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
     if (!t) return MCLCCD_ERR_INVALID;
     t->err.clear();
     if (!t->built) return fail(t, MCLCCD_ERR_STATE, "traverse before a successful update");
-    if (t->flags & MCLCCD_OPT_VF_ONE_SIDED)
-        return fail(t, MCLCCD_ERR_UNSUPPORTED, "vf_one_sided (CTCD narrow phase) is not provided");
     if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
     t->n_pairs = t->n_vf = t->n_ee = t->n_hits = t->n_disc = 0;
     t->traversed = true;
@@ -443,8 +439,14 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
         t->launches += 2;
         if (cont) {
             // FP32-certified: an FP32 pass and an FP64 pass over its queue per list.
+            const bool one_sided = (t->flags & MCLCCD_OPT_VF_ONE_SIDED) != 0;
             auto accd = [&](bool vf, DevBuf &list, unsigned long long *n_ptr, unsigned long long cap, double eta) {
-                if (certified) {
+                if (vf && one_sided) {   // BVHTree.cpp:445-447: CTCD with the wrong-side test
+                    launch_ctcd_pipeline(dim, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
+                                         as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
+                                         t->tune[MCLCCD_TUNE_ACCD_GRID], st);
+                    ++t->launches;
+                } else if (certified) {
                     launch_accd_certified(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
                                           as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits,
                                           as<unsigned>(t->fp64_queue), cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], st);
@@ -623,7 +625,10 @@ int mclccd_narrow_phase_bulk_ex(int dim, const double *V0, const double *V1, int
                                 int *out_hit, int mem_kind, void *stream, int precision, long long *n_fp64)
 {
     if (n_fp64) *n_fp64 = 0;
+    const bool one_sided = (precision & MCLCCD_BULK_VF_ONE_SIDED) != 0;
+    precision &= ~MCLCCD_BULK_VF_ONE_SIDED;
     if (precision != MCLCCD_PREC_FP64 && precision != MCLCCD_PREC_FP32_CERTIFIED) return MCLCCD_ERR_INVALID;
+    if (one_sided && precision != MCLCCD_PREC_FP64) return MCLCCD_ERR_UNSUPPORTED;
     if ((dim != 2 && dim != 3) || n < 0 || nv < 0) return MCLCCD_ERR_INVALID;
     if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return MCLCCD_ERR_INVALID;
     if (!(vf_eta >= 0) || !(ee_eta >= 0)) return MCLCCD_ERR_INVALID;
@@ -672,7 +677,7 @@ int mclccd_narrow_phase_bulk_ex(int dim, const double *V0, const double *V1, int
             launch_accd_certified_bulk(dim, ds, df, n, dV0, dV1, nv, vf_eta, ee_eta, dt, dh,
                                        reinterpret_cast<long long *>(scratch + off_q), cnt, st);
         else
-            launch_accd_bulk(dim, ds, df, n, dV0, dV1, nv, vf_eta, ee_eta, dt, dh, cnt, st);
+            launch_accd_bulk(dim, ds, df, n, dV0, dV1, nv, vf_eta, ee_eta, dt, dh, cnt, st, one_sided);
         e = cudaGetLastError();
     }
     Counters h{};

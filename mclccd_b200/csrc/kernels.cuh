@@ -52,6 +52,10 @@ void launch_vjp_toi(int dim, const int *sten, const unsigned char *is_vf, const 
                     cudaStream_t st);
 void launch_accd_bulk(int dim, const int *sten, const unsigned char *is_vf, long long n, const double *V0,
                       const double *V1, int nv, double vf_eta, double ee_eta, double *out_toi, int *out_hit,
-                      Counters *cnt, cudaStream_t st);
+                      Counters *cnt, cudaStream_t st, bool vf_one_sided = false);
+// narrow.cu: one-sided VF narrow phase (CTCD) over the VF list
+void launch_ctcd_pipeline(int dim, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
+                          const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
+                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st);
 
 } // namespace mclccd

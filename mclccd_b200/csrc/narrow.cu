@@ -6,6 +6,7 @@
 // append hits to the compacted contact buffer (warp-aggregated) or write the
 // per-stencil (toi, hit) of the bulk call.  Compiled with -fmad=false.
 #include "common.cuh"
+#include "ctcd.cuh"
 #include "geom.cuh"
 #include "kernels.cuh"
 
@@ -185,9 +186,50 @@ k_accd_rebin(const int4 *__restrict__ sten, const unsigned long long *n_ptr, uns
     }
 }
 
+// One-sided VF narrow phase (CTCD with the wrong-side test): 1 hit, 0 no
+// contact, -1 only wrong-side contacts.
+template <int DIM>
+__device__ __forceinline__ int ctcd_vf(const double (&x0)[DIM + 1][DIM], const double (&x1)[DIM + 1][DIM], double eta,
+                                       double &toi)
+{
+    if constexpr (DIM == 3) return ctcd::query_vf3(x0, x1, eta, toi);
+    else return ctcd::query_vf2(x0, x1, toi);
+}
+
+// Pipeline form of the one-sided VF narrow phase (vf_one_sided): the VF
+// list of the expansion kernel -> compacted hits.
+template <int DIM>
+__global__ void __launch_bounds__(128)
+k_ctcd_pipeline(const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
+                const double *__restrict__ V0, const double *__restrict__ V1, int nv, double eta,
+                int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,
+                unsigned long long hit_cap, Counters *cnt)
+{
+    unsigned long long n = *(volatile const unsigned long long *)n_ptr;
+    if (n > cap) n = cap;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int4 s4 = sten[i];
+        const int s[4] = {s4.x, s4.y, s4.z, s4.w};
+        double x0[DIM + 1][DIM], x1[DIM + 1][DIM];
+        if (!gather_stencil<DIM>(s, V0, V1, nv, x0, x1)) { atomicOr(&cnt->err, kErrBadIndex); continue; }
+        double toi = -1.0;
+        // default_narrow_phase keeps ret == 1 only; collide() needs toi >= 0
+        if (ctcd_vf<DIM>(x0, x1, eta, toi) == 1 && toi >= 0.0) {
+            const unsigned long long slot = warp_append(&cnt->n_hits);
+            if (slot < hit_cap) {
+                hit_sten[slot] = s4;
+                hit_toi[slot] = toi;
+                hit_isvf[slot] = 1;
+            }
+        }
+    }
+}
+
 // Bulk form: caller-given stencils (int32 x 4 each, any alignment), per-stencil
 // outputs in input order.  toi = -1 on a miss, as default_narrow_phase returns.
-template <int DIM>
+// ONE_SIDED: VF stencils take the CTCD one-sided narrow phase.
+template <int DIM, bool ONE_SIDED>
 __global__ void __launch_bounds__(128)
 k_accd_bulk(const int *__restrict__ sten, const unsigned char *__restrict__ is_vf, long long n,
             const double *__restrict__ V0, const double *__restrict__ V1, int nv, double vf_eta, double ee_eta,
@@ -203,6 +245,8 @@ k_accd_bulk(const int *__restrict__ sten, const unsigned char *__restrict__ is_v
             atomicOr(&cnt->err, kErrBadIndex);
         } else if (DIM == 3 && !is_vf[i]) {
             hit = accd<DIM, false>(x0, x1, ee_eta, toi, iters);
+        } else if (ONE_SIDED) {
+            hit = ctcd_vf<DIM>(x0, x1, vf_eta, toi) == 1 ? 1 : 0;
         } else {
             hit = accd<DIM, true>(x0, x1, vf_eta, toi, iters);
         }
@@ -236,13 +280,26 @@ void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned lon
 
 void launch_accd_bulk(int dim, const int *sten, const unsigned char *is_vf, long long n, const double *V0,
                       const double *V1, int nv, double vf_eta, double ee_eta, double *out_toi, int *out_hit,
-                      Counters *cnt, cudaStream_t st)
+                      Counters *cnt, cudaStream_t st, bool vf_one_sided)
 {
     if (n <= 0) return;
     long long g = (n + 127) / 128;
     if (g > 148 * 32) g = 148 * 32;
-    if (dim == 3) k_accd_bulk<3><<<(int)g, 128, 0, st>>>(sten, is_vf, n, V0, V1, nv, vf_eta, ee_eta, out_toi, out_hit, cnt);
-    else k_accd_bulk<2><<<(int)g, 128, 0, st>>>(sten, is_vf, n, V0, V1, nv, vf_eta, ee_eta, out_toi, out_hit, cnt);
+    if (vf_one_sided) {
+        if (dim == 3) k_accd_bulk<3, true><<<(int)g, 128, 0, st>>>(sten, is_vf, n, V0, V1, nv, vf_eta, ee_eta, out_toi, out_hit, cnt);
+        else k_accd_bulk<2, true><<<(int)g, 128, 0, st>>>(sten, is_vf, n, V0, V1, nv, vf_eta, ee_eta, out_toi, out_hit, cnt);
+        return;
+    }
+    if (dim == 3) k_accd_bulk<3, false><<<(int)g, 128, 0, st>>>(sten, is_vf, n, V0, V1, nv, vf_eta, ee_eta, out_toi, out_hit, cnt);
+    else k_accd_bulk<2, false><<<(int)g, 128, 0, st>>>(sten, is_vf, n, V0, V1, nv, vf_eta, ee_eta, out_toi, out_hit, cnt);
+}
+
+void launch_ctcd_pipeline(int dim, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
+                          const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
+                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st)
+{
+    if (dim == 3) k_ctcd_pipeline<3><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+    else k_ctcd_pipeline<2><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
 }
 
 } // namespace mclccd

@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libmclccd_ref.so")
 PORT_SO = os.path.join(HERE, "_build", "liboracle_port.so")
 
-F_REPTRI, F_THREADED, F_DISCRETE, F_CONTINUOUS, F_RECORD_CAND = 1, 2, 4, 8, 16
+F_REPTRI, F_THREADED, F_DISCRETE, F_CONTINUOUS, F_RECORD_CAND, F_ONE_SIDED = 1, 2, 4, 8, 16, 32
 DEFAULT_FLAGS = F_REPTRI | F_THREADED | F_DISCRETE | F_CONTINUOUS
 
 
@@ -77,6 +77,9 @@ class Reference:
         L.ref_copy_leaves.argtypes = [_dp, _ip]
         L.ref_accd.argtypes = [C.c_int, _dp, _dp, _ip, _ucp, C.c_longlong, C.c_double, C.c_double, _ip, _dp]
         L.ref_discrete.argtypes = [C.c_int, _dp, _ip, _ip, C.c_longlong, _ip]
+        L.ref_ctcd_vf.argtypes = [C.c_int, _dp, _dp, _ip, C.c_longlong, C.c_double, _ip, _dp]
+        L.ref_rpoly.argtypes = [_dp, C.c_int, _dp, _dp]
+        L.ref_rpoly.restype = C.c_int
         L.ref_time.argtypes = [C.c_int, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_double, C.c_int,
                                _dp, _dp, _dp, C.POINTER(C.c_longlong)]
         L.ref_time.restype = C.c_longlong
@@ -117,6 +120,27 @@ class Reference:
         self.L.ref_accd(V0.shape[1], _p(V0, C.c_double), _p(V1, C.c_double), _p(s, C.c_int), _p(v, C.c_ubyte), n,
                         vf_eta, vf_eta if ee_eta is None else ee_eta, _p(hit, C.c_int), _p(toi, C.c_double))
         return hit, toi
+
+    def ctcd_vf(self, V0, V1, sten, eta):
+        """The reference's NarrowPhaseCTCD::query_ccd_vf with the wrong-side
+        test, per stencil: (ret, toi); ret 1 hit, 0 none, -1 wrong side only."""
+        V0 = np.ascontiguousarray(V0, np.float64)
+        V1 = np.ascontiguousarray(V1, np.float64)
+        s = np.ascontiguousarray(sten, np.int32).reshape(-1, 4)
+        n = len(s)
+        ret = np.empty(n, np.int32); toi = np.empty(n, np.float64)
+        self.L.ref_ctcd_vf(V0.shape[1], _p(V0, C.c_double), _p(V1, C.c_double), _p(s, C.c_int), n, eta,
+                           _p(ret, C.c_int), _p(toi, C.c_double))
+        return ret, toi
+
+    def rpoly(self, op):
+        """The reference's Jenkins-Traub root finder on op (descending
+        powers): complex roots as a numpy array (root count it reports)."""
+        c = np.array(op, np.float64)
+        n = len(c) - 1
+        re = np.zeros(n); im = np.zeros(n)
+        k = self.L.ref_rpoly(_p(c, C.c_double), n, _p(re, C.c_double), _p(im, C.c_double))
+        return (re + 1j * im)[:max(k, 0)]
 
     def discrete(self, V, F, pairs):
         V = np.ascontiguousarray(V, np.float64)

@@ -14,6 +14,7 @@
 // through sharded, mutex-protected buffers.
 #include "MCL/BVHTree.hpp"
 #include "MCL/NarrowPhase.hpp"
+#include "MCL/ccd_internal/rpoly.h"
 #include "tbb/parallel_for.h"
 
 #include <atomic>
@@ -59,7 +60,7 @@ struct State {
 };
 State g_state;
 
-enum { F_REPTRI = 1, F_THREADED = 2, F_DISCRETE = 4, F_CONTINUOUS = 8, F_RECORD_CAND = 16 };
+enum { F_REPTRI = 1, F_THREADED = 2, F_DISCRETE = 4, F_CONTINUOUS = 8, F_RECORD_CAND = 16, F_ONE_SIDED = 32 };
 
 template <int DIM>
 int run(const double *V0, const double *V1, const int *P, int np, int pdim,
@@ -73,6 +74,7 @@ int run(const double *V0, const double *V1, const int *P, int np, int pdim,
     tree.options.threaded = (flags & F_THREADED) != 0;
     tree.options.discrete = (flags & F_DISCRETE) != 0;
     tree.options.continuous = (flags & F_CONTINUOUS) != 0;
+    tree.options.vf_one_sided = (flags & F_ONE_SIDED) != 0;
 
     Sharded<Candidate> cand;
     Sharded<Hit> hits;
@@ -137,9 +139,48 @@ void accd(const double *V0, const double *V1, const int *sten, const unsigned ch
     }
 }
 
+// NarrowPhaseCTCD::query_ccd_vf (NarrowPhase.cpp:282-333 in 2D, 338-425 in
+// 3D) with test_wrong_side = true, as default_narrow_phase calls it when
+// vf_one_sided is set (BVHTree.cpp:445-447).  ret: 1 hit, 0 no hit, -1 only
+// wrong-side hits; toi = t_impact on a hit, -1 otherwise.
+template <int DIM>
+void ctcd_vf(const double *V0, const double *V1, const int *sten, long long n, double eta, int *ret, double *toi)
+{
+    typedef typename mcl::NarrowPhaseCTCD<double, DIM>::VecType Vec;
+    for (long long s = 0; s < n; ++s) {
+        Vec x0[DIM + 1], x1[DIM + 1];
+        for (int i = 0; i < DIM + 1; ++i)
+            for (int k = 0; k < DIM; ++k) {
+                x0[i][k] = V0[size_t(sten[4 * s + i]) * DIM + k];
+                x1[i][k] = V1[size_t(sten[4 * s + i]) * DIM + k];
+            }
+        double t = -1;
+        const int h = mcl::NarrowPhaseCTCD<double, DIM>::query_ccd_vf(x0, x1, eta, true, t);
+        ret[s] = h;
+        toi[s] = h == 1 ? t : -1.0;
+    }
+}
+
 } // namespace
 
 extern "C" {
+
+// The reference's polynomial root finder (ccd_internal/rpoly.h, a
+// Jenkins-Traub RPOLY), as findIntervals calls it (CTCD.cpp:148): op in
+// descending powers (modified in place, as the reference lets it), all
+// roots' real and imaginary parts.  Returns its root count.
+int ref_rpoly(double *op, int degree, double *re, double *im)
+{
+    mcl::RootFinder rf;
+    return rf.rpoly(op, degree, re, im);
+}
+
+void ref_ctcd_vf(int dim, const double *V0, const double *V1, const int *sten, long long n, double eta, int *ret,
+                 double *toi)
+{
+    if (dim == 3) ctcd_vf<3>(V0, V1, sten, n, eta, ret, toi);
+    else ctcd_vf<2>(V0, V1, sten, n, eta, ret, toi);
+}
 
 // update(V0,V1,P) + traverse(V0,V1,P) with recording hooks.  flags: see F_*.
 int ref_run(int dim, const double *V0, const double *V1, const int *P, int np, int pdim,

@@ -223,10 +223,6 @@ def test_empty_single_and_errors():
     with pytest.raises(CCDError) as e:
         bad.update(V, V, np.array([[0, 1, 7], [0, 1, 2]], np.int32))
     assert e.value.status == 1   # index out of range
-    bad.options.vf_one_sided = True
-    with pytest.raises(CCDError) as e:
-        bad.update(V, V, np.array([[0, 1, 2]], np.int32))
-    assert e.value.status == 7
 
 
 def test_bulk_narrow_phase_matches_port(port):

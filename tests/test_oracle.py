@@ -114,3 +114,39 @@ def test_port_edge_cases(port):
     V2b[3:, 2] = -0.1                                                     # sweeps through triangle 0
     d = port.run(V2, V2b, F2, 1e-3)
     assert len(d["cand_sten"]) > 0 and len(d["hit_sten"]) > 0
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference oracle not built")
+def test_reference_ctcd_one_sided_cases():
+    # the reference's own one-sided VF narrow phase (the checker of the device
+    # CTCD): a fall onto the face from above hits when the gap reaches eta, a
+    # rise from below is a wrong-side contact, parallel or outside motion misses
+    R = Reference()
+    eta = 1e-3
+    tri = [[0, 0, 0], [1, 0, 0], [0, 1, 0]]
+    V0 = np.array([[0.2, 0.2, 0.5]] + tri + [[0.2, 0.2, -0.5]] + tri + [[0.2, 0.2, 0.5]] + tri + [[1, 1, 0.5]] + tri,
+                  float)
+    V1 = V0.copy()
+    V1[0, 2], V1[4, 2], V1[8, 0], V1[12, 2] = -0.5, 0.5, 0.7, -0.5
+    ret, toi = R.ctcd_vf(V0, V1, np.arange(16, dtype=np.int32).reshape(4, 4), eta)
+    assert list(ret) == [1, -1, 0, 0]
+    assert abs(toi[0] - (0.5 - eta)) < 1e-12
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference oracle not built")
+def test_reference_rpoly_matches_eigenvalue_roots():
+    # the reference's Jenkins-Traub root finder (the one the device CTCD's
+    # Aberth iteration stands in for) agrees with companion-matrix eigenvalues
+    # on well-separated roots, degrees 3-6
+    R = Reference()
+    rng = np.random.default_rng(5)
+    for deg in range(3, 7):
+        for _ in range(50):
+            pairs = deg // 3   # complex-conjugate pairs, the rest real
+            z = rng.uniform(-2, 2, pairs) + 1j * rng.uniform(0.2, 1.0, pairs)
+            roots = np.concatenate([rng.uniform(-2, 2, deg - 2 * pairs), z, np.conj(z)])
+            op = np.real(np.poly(roots))
+            got = R.rpoly(op)
+            want = np.roots(op)
+            assert len(got) == deg
+            assert all(np.min(np.abs(want - g)) < 1e-8 for g in got), (got, want)
