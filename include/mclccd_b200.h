@@ -284,6 +284,17 @@ typedef struct {
 } mclccd_tree_view;
 int mclccd_get_tree_view(const mclccd_tree *tree, mclccd_tree_view *view);
 
+/* float coordinates (the reference's BVHTree<float, DIM> instantiations,
+ * BVHTree.cpp:506-507): V0/V1 are float (nv x dim, mem_kind side) and are
+ * widened exactly to double on the device, then update / traverse run as
+ * mclccd_update / mclccd_traverse on those doubles.  Results are therefore
+ * the FP64 path's results for these coordinates (toi as double; the C++
+ * BVHTree<float, DIM> rounds it down to float).  traverse_f32 with all
+ * arrays NULL reuses the last update's. */
+int mclccd_update_f32(mclccd_tree *tree, const float *V0, const float *V1, int nv, const int *P, int np, int pdim,
+                      const int *active, int mem_kind);
+int mclccd_traverse_f32(mclccd_tree *tree, const float *V0, const float *V1, int nv, const int *P, int mem_kind);
+
 /* Per-stage device times (ms) of the last update + traverse when
  * MCLCCD_OPT_PROFILE is set: [update_total, build, refit, traverse_total,
  * tree_walk, expand, narrow]; returns how many were written. */

@@ -1,6 +1,9 @@
-// Drop-in C++ replacement for mclccd's mcl::BVHTree<double, DIM>
-// (include/MCL/BVHTree.hpp), running the CCD path on the GPU through the C ABI
-// in include/mclccd_b200.h.  Link with libmclccd_b200.so.
+// Drop-in C++ replacement for mclccd's mcl::BVHTree<T, DIM>, T = double or
+// float, DIM = 2 or 3 (include/MCL/BVHTree.hpp; instantiations
+// BVHTree.cpp:504-507), running the CCD path on the GPU through the C ABI in
+// include/mclccd_b200.h.  Link with libmclccd_b200.so.  float trees widen
+// their coordinates exactly to double on the device and run the FP64 path;
+// their toi is that FP64 toi rounded down to float (never later).
 //
 // Same members as the reference: Options (same fields and defaults),
 // update(), traverse(), and the hooks append_pair, append_discrete,
@@ -19,6 +22,9 @@
 
 #include <algorithm>
 #include <array>
+#include <cmath>
+#include <limits>
+#include <type_traits>
 #include <functional>
 #include <stdexcept>
 #include <string>
@@ -46,17 +52,17 @@ public:
 };
 
 template <typename T, int DIM>
-class BVHTree;
-
-template <int DIM>
-class BVHTree<double, DIM> {
-    static_assert(DIM == 2 || DIM == 3, "mcl::BVHTree<double, DIM>: DIM must be 2 or 3");
+class BVHTree {
+    static_assert(DIM == 2 || DIM == 3, "mcl::BVHTree<T, DIM>: DIM must be 2 or 3");
+    static_assert(std::is_same<T, double>::value || std::is_same<T, float>::value,
+                  "mcl::BVHTree<T, DIM>: T must be double or float");
+    static constexpr bool kFloat = std::is_same<T, float>::value;
 
 public:
     struct Options {
-        double box_eta = 1e-6;     // padding of tree boxes
-        double vf_ccd_eta = 1e-6;  // gap for vf narrowphase <= box_eta
-        double ee_ccd_eta = 1e-6;  // gap for ee narrowphase <= box_eta
+        T box_eta = T(1e-6);     // padding of tree boxes
+        T vf_ccd_eta = T(1e-6);  // gap for vf narrowphase <= box_eta
+        T ee_ccd_eta = T(1e-6);  // gap for ee narrowphase <= box_eta
         bool reptri = true;        // representative triangles
         bool threaded = true;      // accepted; the GPU path is always parallel
         bool discrete = true;      // discrete check ff/ee at V1
@@ -65,10 +71,10 @@ public:
         bool ee_robust = true;     // unused by ACCD, as in the reference
     } options;
 
-    std::function<void(const Stencil &sten, bool is_vf, const double &toi)> append_pair;
+    std::function<void(const Stencil &sten, bool is_vf, const T &toi)> append_pair;
     std::function<bool(int p0, int p1)> append_discrete;
     std::function<bool(const Stencil &sten, bool is_vf)> filter_pair;
-    std::function<double(const Stencil &sten, bool is_vf)> narrow_phase;
+    std::function<T(const Stencil &sten, bool is_vf)> narrow_phase;
 
     BVHTree() { check(mclccd_create(DIM, &h_)); }
     ~BVHTree() { if (h_) mclccd_destroy(h_); }
@@ -77,7 +83,7 @@ public:
 
     // Reference signature (BVHTree.hpp:81-82).  It carries no vertex count, so
     // the count is taken as 1 + the largest index in P.
-    void update(const double *V0, const double *V1, const int *P, int np, int pdim, const int *active = nullptr)
+    void update(const T *V0, const T *V1, const int *P, int np, int pdim, const int *active = nullptr)
     {
         int nv = 0;
         for (long long i = 0; i < (long long)np * pdim; ++i) nv = std::max(nv, P[i] + 1);
@@ -86,11 +92,13 @@ public:
 
     // With an explicit vertex count; mem_kind MCLCCD_MEM_DEVICE takes device
     // pointers (no host copies at all).
-    void update(const double *V0, const double *V1, int nv, const int *P, int np, int pdim, const int *active,
+    void update(const T *V0, const T *V1, int nv, const int *P, int np, int pdim, const int *active,
                 int mem_kind)
     {
         push_options();
-        int rc = mclccd_update(h_, V0, V1, nv, P, np, pdim, active, mem_kind);
+        int rc;
+        if constexpr (kFloat) rc = mclccd_update_f32(h_, V0, V1, nv, P, np, pdim, active, mem_kind);
+        else rc = mclccd_update(h_, V0, V1, nv, P, np, pdim, active, mem_kind);
         pull_options();
         check(rc);
         nv_ = nv;
@@ -100,11 +108,12 @@ public:
 
     // Reference signature (BVHTree.hpp:86).  Runs the device pipeline on the
     // given arrays (same side as the last update), then calls the hooks.
-    void traverse(const double *V0, const double *V1, const int *P) const
+    void traverse(const T *V0, const T *V1, const int *P) const
     {
         auto *self = const_cast<BVHTree *>(this);
         self->push_options();
-        check(mclccd_traverse(h_, V0, V1, nv_, P, mem_));
+        if constexpr (kFloat) check(mclccd_traverse_f32(h_, V0, V1, nv_, P, mem_));
+        else check(mclccd_traverse(h_, V0, V1, nv_, P, mem_));
         self->dispatch(V0, V1);
     }
 
@@ -113,7 +122,8 @@ public:
     {
         auto *self = const_cast<BVHTree *>(this);
         self->push_options();
-        check(mclccd_traverse(h_, nullptr, nullptr, 0, nullptr, mem_));
+        if constexpr (kFloat) check(mclccd_traverse_f32(h_, nullptr, nullptr, 0, nullptr, mem_));
+        else check(mclccd_traverse(h_, nullptr, nullptr, 0, nullptr, mem_));
         self->dispatch(nullptr, nullptr);
     }
 
@@ -125,7 +135,7 @@ public:
                 const Eigen::MatrixBase<DerivedP> &P, const Eigen::VectorXi &active = Eigen::VectorXi())
     {
         if (V0.rows() != V1.rows()) throw CCDError(MCLCCD_ERR_INVALID, "V0 and V1 row counts differ");
-        RowV v0 = V0.template cast<double>(), v1 = V1.template cast<double>();
+        RowV v0 = V0.template cast<T>(), v1 = V1.template cast<T>();
         RowP p = P.template cast<int>();
         const int *act = active.size() == V0.rows() ? active.data() : nullptr;
         update(v0.data(), v1.data(), (int)v0.rows(), p.data(), (int)p.rows(), (int)p.cols(), act, MCLCCD_MEM_HOST);
@@ -135,7 +145,7 @@ public:
                   const Eigen::MatrixBase<DerivedP> &P)
     {
         if (V0.rows() != V1.rows()) throw CCDError(MCLCCD_ERR_INVALID, "V0 and V1 row counts differ");
-        RowV v0 = V0.template cast<double>(), v1 = V1.template cast<double>();
+        RowV v0 = V0.template cast<T>(), v1 = V1.template cast<T>();
         RowP p = P.template cast<int>();
         traverse(v0.data(), v1.data(), p.data());
     }
@@ -167,7 +177,7 @@ public:
 
 private:
 #ifdef MCLCCD_B200_HAVE_EIGEN
-    typedef Eigen::Matrix<double, Eigen::Dynamic, DIM, Eigen::RowMajor> RowV;
+    typedef Eigen::Matrix<T, Eigen::Dynamic, DIM, Eigen::RowMajor> RowV;
     typedef Eigen::Matrix<int, Eigen::Dynamic, Eigen::Dynamic, Eigen::RowMajor> RowP;
 #endif
     mclccd_tree *h_ = nullptr;
@@ -189,11 +199,27 @@ private:
         if (options.continuous) f |= MCLCCD_OPT_CONTINUOUS;
         if (options.vf_one_sided) f |= MCLCCD_OPT_VF_ONE_SIDED;
         if (options.ee_robust) f |= MCLCCD_OPT_EE_ROBUST;
-        check(mclccd_set_options(h_, options.box_eta, options.vf_ccd_eta, options.ee_ccd_eta, f));
+        check(mclccd_set_options(h_, (double)options.box_eta, (double)options.vf_ccd_eta, (double)options.ee_ccd_eta,
+                                 f));
     }
     void pull_options()
     {
-        mclccd_get_options(h_, &options.box_eta, &options.vf_ccd_eta, &options.ee_ccd_eta, nullptr);
+        double b = 0, v = 0, e = 0;
+        mclccd_get_options(h_, &b, &v, &e, nullptr);
+        options.box_eta = (T)b;
+        options.vf_ccd_eta = (T)v;
+        options.ee_ccd_eta = (T)e;
+    }
+    // A device toi (double) as T: float rounds down, so it is never later.
+    static T to_toi(double t)
+    {
+        if constexpr (kFloat) {
+            float f = (float)t;
+            if ((double)f > t) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+            return f;
+        } else {
+            return t;
+        }
     }
     static Stencil make_stencil(const int *s)
     {
@@ -201,7 +227,7 @@ private:
         for (int i = 0; i < 4; ++i) t[i] = s[i];
         return t;
     }
-    void dispatch(const double *V0, const double *V1)
+    void dispatch(const T *V0, const T *V1)
     {
         if (filter_pair || narrow_phase) {
             std::vector<int> cs;
@@ -221,19 +247,32 @@ private:
                 if (!V0 || mem_ != MCLCCD_MEM_HOST)
                     throw CCDError(MCLCCD_ERR_INVALID, "filter_pair without narrow_phase needs host V0/V1 at traverse");
                 std::vector<int> hit(kv.size());
-                check(mclccd_narrow_phase_bulk(DIM, V0, V1, nv_, ks.data(), kv.data(), (long long)kv.size(),
-                                               options.vf_ccd_eta, options.ee_ccd_eta, toi.data(), hit.data(),
-                                               MCLCCD_MEM_HOST, nullptr));
+                const double *v0 = nullptr, *v1 = nullptr;
+                std::vector<double> w0, w1;
+                if constexpr (kFloat) {
+                    w0.assign(V0, V0 + (size_t)nv_ * DIM);
+                    w1.assign(V1, V1 + (size_t)nv_ * DIM);
+                    v0 = w0.data();
+                    v1 = w1.data();
+                } else {
+                    v0 = V0;
+                    v1 = V1;
+                }
+                check(mclccd_narrow_phase_bulk_ex(DIM, v0, v1, nv_, ks.data(), kv.data(), (long long)kv.size(),
+                                                  (double)options.vf_ccd_eta, (double)options.ee_ccd_eta, toi.data(),
+                                                  hit.data(), MCLCCD_MEM_HOST, nullptr,
+                                                  MCLCCD_PREC_FP64 | (options.vf_one_sided ? MCLCCD_BULK_VF_ONE_SIDED : 0),
+                                                  nullptr));
             }
             if (append_pair)
                 for (size_t i = 0; i < kv.size(); ++i)
-                    if (toi[i] >= 0) append_pair(make_stencil(&ks[4 * i]), kv[i] != 0, toi[i]);
+                    if (toi[i] >= 0) append_pair(make_stencil(&ks[4 * i]), kv[i] != 0, to_toi(toi[i]));
         } else if (append_pair) {
             std::vector<int> s;
             std::vector<unsigned char> v;
             std::vector<double> t;
             hits(s, v, t);
-            for (size_t i = 0; i < v.size(); ++i) append_pair(make_stencil(&s[4 * i]), v[i] != 0, t[i]);
+            for (size_t i = 0; i < v.size(); ++i) append_pair(make_stencil(&s[4 * i]), v[i] != 0, to_toi(t[i]));
         }
         if (append_discrete && options.discrete) {
             std::vector<int> d;

@@ -63,6 +63,8 @@ def lib():
         "mclccd_set_precision": ([vp, C.c_int], C.c_int),
         "mclccd_update": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int], C.c_int),
         "mclccd_traverse": ([vp, vp, vp, C.c_int, vp, C.c_int], C.c_int),
+        "mclccd_update_f32": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int], C.c_int),
+        "mclccd_traverse_f32": ([vp, vp, vp, C.c_int, vp, C.c_int], C.c_int),
         "mclccd_counts": ([vp, llp, llp, llp, llp, llp], C.c_int),
         "mclccd_get_hits": ([vp, C.c_int, C.c_longlong, vp, vp, vp], C.c_int),
         "mclccd_get_discrete": ([vp, C.c_int, C.c_longlong, vp], C.c_int),
@@ -95,13 +97,23 @@ def _is_torch_cuda(a) -> bool:
     return type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False)
 
 
+def _is_f32(a):
+    """float32 coordinates (numpy array or CUDA tensor)."""
+    if a is None:
+        return False
+    if _is_torch_cuda(a):
+        import torch
+        return a.dtype == torch.float32
+    return getattr(a, "dtype", None) == np.float32
+
+
 def _arg(a, dtype, cols=None):
     """(pointer, mem_kind, keepalive, rows) for a numpy array or CUDA tensor."""
     if a is None:
         return None, None, None, 0
     if _is_torch_cuda(a):
         import torch
-        tdt = {np.float64: torch.float64, np.int32: torch.int32, np.uint8: torch.uint8}[dtype]
+        tdt = {np.float64: torch.float64, np.float32: torch.float32, np.int32: torch.int32, np.uint8: torch.uint8}[dtype]
         if a.dtype != tdt:
             raise TypeError(f"expected {tdt}, got {a.dtype}")
         a = a.contiguous()
@@ -210,9 +222,13 @@ class BVHTree:
 
     # -- the reference API --------------------------------------------------
     def update(self, V0, V1, P, active=None):
-        """BVHTree::update (BVHTree.cpp:27-126)."""
-        pv0, k0, a0, nv = _arg(V0, np.float64, self.dim)
-        pv1, k1, a1, nv1 = _arg(V1, np.float64, self.dim)
+        """BVHTree::update (BVHTree.cpp:27-126).  float32 coordinates take
+        the BVHTree<float, DIM> form (mclccd_update_f32: widened exactly to
+        double on the device)."""
+        f32 = _is_f32(V0)
+        vt = np.float32 if f32 else np.float64
+        pv0, k0, a0, nv = _arg(V0, vt, self.dim)
+        pv1, k1, a1, nv1 = _arg(V1, vt, self.dim)
         pp, kp, ap, npr = _arg(P, np.int32)
         pa, ka, aa, _ = _arg(active, np.int32)
         if nv != nv1:   # BVHTree.hpp:160: silently ignored by the reference
@@ -222,7 +238,8 @@ class BVHTree:
             raise ValueError("V0, V1, P and active must all be host arrays or all CUDA tensors")
         pdim = ap.shape[1] if ap.ndim == 2 else self.dim
         self._push_options()
-        rc = self._L.mclccd_update(self._h, pv0, pv1, nv, pp, npr, pdim, pa, kinds.pop() if kinds else MEM_HOST)
+        upd = self._L.mclccd_update_f32 if f32 else self._L.mclccd_update
+        rc = upd(self._h, pv0, pv1, nv, pp, npr, pdim, pa, kinds.pop() if kinds else MEM_HOST)
         self._pull_options()
         self._check(rc, self._h)
         self._keep = [a0, a1, ap, aa]
@@ -230,12 +247,15 @@ class BVHTree:
 
     def traverse(self, V0=None, V1=None, P=None):
         """BVHTree::traverse (BVHTree.cpp:129-159), then the hooks."""
-        pv0, k0, a0, nv = _arg(V0, np.float64, self.dim)
-        pv1, k1, a1, _ = _arg(V1, np.float64, self.dim)
+        f32 = _is_f32(V0)
+        vt = np.float32 if f32 else np.float64
+        pv0, k0, a0, nv = _arg(V0, vt, self.dim)
+        pv1, k1, a1, _ = _arg(V1, vt, self.dim)
         pp, kp, ap, _ = _arg(P, np.int32)
         kind = k0 if k0 is not None else MEM_HOST
         self._push_options()
-        self._check(self._L.mclccd_traverse(self._h, pv0, pv1, nv, pp, kind), self._h)
+        trv = self._L.mclccd_traverse_f32 if f32 else self._L.mclccd_traverse
+        self._check(trv(self._h, pv0, pv1, nv, pp, kind), self._h)
         if V0 is not None:
             self._nv = nv
         self._dispatch(V0, V1)

@@ -58,12 +58,13 @@ struct mclccd_tree {
     DevBuf cent, bounds, keys, vals, keys_alt, vals_alt, sort_scratch;
     DevBuf nodes, leaf_parent, visits, leaf_box, leaf_active;
     DevBuf pairs, vf, ee, hit_sten, hit_toi, hit_isvf, disc, counters, diff, fp64_queue;
+    DevBuf f32_V, f32_P, f32_act;   // float-input staging (mclccd_update_f32 / mclccd_traverse_f32)
     std::vector<DevBuf *> all()
     {
         return {&V0d, &V1d, &Pd, &Pstage, &actd, &pflags, &pflags_tmp, &vowner, &ekeys, &eowner, &cent, &bounds,
                 &keys, &vals, &keys_alt, &vals_alt, &sort_scratch, &nodes, &leaf_parent, &visits, &leaf_box,
                 &leaf_active, &pairs, &vf, &ee, &hit_sten, &hit_toi, &hit_isvf, &disc, &counters, &diff,
-                &fp64_queue};
+                &fp64_queue, &f32_V, &f32_P, &f32_act};
     }
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
@@ -355,6 +356,86 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
     t->built = derr == 0;
     if (derr) return device_errors(t, derr);
     return MCLCCD_OK;
+}
+
+// float inputs: exact widening to the FP64 arrays the path runs on.
+__global__ void k_widen(const float *__restrict__ a, const float *__restrict__ b, double *__restrict__ oa,
+                        double *__restrict__ ob, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        oa[i] = (double)a[i];
+        ob[i] = (double)b[i];
+    }
+}
+
+// V0/V1 (float, mem_kind side) -> t->V0d/V1d (double, device).
+static int widen_positions(mclccd_tree *t, const float *V0, const float *V1, int nv, int mem_kind)
+{
+    const long long n = (long long)nv * t->dim;
+    cudaStream_t st = t->stream;
+    MC_CUDA(t, ensure(t->V0d, sizeof(double) * (size_t)n));
+    MC_CUDA(t, ensure(t->V1d, sizeof(double) * (size_t)n));
+    const float *a = V0, *b = V1;
+    if (mem_kind == MCLCCD_MEM_HOST) {
+        MC_CUDA(t, ensure(t->f32_V, 2 * sizeof(float) * (size_t)n));
+        float *s = as<float>(t->f32_V);
+        MC_CUDA(t, cudaMemcpyAsync(s, V0, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st));
+        MC_CUDA(t, cudaMemcpyAsync(s + n, V1, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st));
+        a = s;
+        b = s + n;
+    }
+    const long long g = std::min<long long>((n + 255) / 256, 148 * 16);
+    k_widen<<<(int)std::max<long long>(g, 1), 256, 0, st>>>(a, b, as<double>(t->V0d), as<double>(t->V1d), n);
+    ++t->launches;
+    MC_CUDA(t, cudaGetLastError());
+    return MCLCCD_OK;
+}
+
+// An int array on the mem_kind side -> a device pointer (staged when host).
+static int stage_ints(mclccd_tree *t, DevBuf &buf, const int *src, size_t count, int mem_kind, const int *&out)
+{
+    out = src;
+    if (!src || mem_kind != MCLCCD_MEM_HOST) return MCLCCD_OK;
+    MC_CUDA(t, ensure(buf, sizeof(int) * std::max<size_t>(count, 1)));
+    MC_CUDA(t, cudaMemcpyAsync(buf.p, src, sizeof(int) * count, cudaMemcpyHostToDevice, t->stream));
+    out = as<int>(buf);
+    return MCLCCD_OK;
+}
+
+int mclccd_update_f32(mclccd_tree *t, const float *V0, const float *V1, int nv, const int *P, int np, int pdim,
+                      const int *active, int mem_kind)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    t->err.clear();
+    if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
+    if (np < 0 || nv < 0) return fail(t, MCLCCD_ERR_INVALID, "negative size");
+    if (np == 0) return mclccd_update(t, nullptr, nullptr, nv, nullptr, 0, pdim, nullptr, MCLCCD_MEM_DEVICE);
+    if (!V0 || !V1 || !P || nv <= 0) return fail(t, MCLCCD_ERR_INVALID, "null array or nv == 0");
+    if (pdim < 1 || pdim > 4) return fail(t, MCLCCD_ERR_INVALID, "pdim must be in [1, 4]");
+    DeviceGuard g(t->device);
+    const int *dP = nullptr, *dact = nullptr;
+    if (int rc = widen_positions(t, V0, V1, nv, mem_kind)) return rc;
+    if (int rc = stage_ints(t, t->f32_P, P, (size_t)np * pdim, mem_kind, dP)) return rc;
+    if (int rc = stage_ints(t, t->f32_act, active, (size_t)nv, mem_kind, dact)) return rc;
+    return mclccd_update(t, as<double>(t->V0d), as<double>(t->V1d), nv, dP, np, pdim, dact, MCLCCD_MEM_DEVICE);
+}
+
+int mclccd_traverse_f32(mclccd_tree *t, const float *V0, const float *V1, int nv, const int *P, int mem_kind)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    t->err.clear();
+    if (!V0 && !V1 && !P) return mclccd_traverse(t, nullptr, nullptr, 0, nullptr, MCLCCD_MEM_DEVICE);
+    if (!V0 || !V1 || !P) return fail(t, MCLCCD_ERR_INVALID, "V0, V1, P must all be given (or all NULL)");
+    if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
+    if (!t->built) return fail(t, MCLCCD_ERR_STATE, "traverse before a successful update");
+    if (nv <= 0) nv = t->nv;
+    DeviceGuard g(t->device);
+    const int *dP = nullptr;
+    if (int rc = widen_positions(t, V0, V1, nv, mem_kind)) return rc;
+    if (int rc = stage_ints(t, t->f32_P, P, (size_t)t->np * t->dim, mem_kind, dP)) return rc;
+    t->upd_V0 = as<double>(t->V0d);   // the update's arrays were overwritten
+    t->upd_V1 = as<double>(t->V1d);
+    return mclccd_traverse(t, as<double>(t->V0d), as<double>(t->V1d), nv, dP, MCLCCD_MEM_DEVICE);
 }
 
 int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, const int *P, int mem_kind)

@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libmclccd_ref.so")
 PORT_SO = os.path.join(HERE, "_build", "liboracle_port.so")
 
-F_REPTRI, F_THREADED, F_DISCRETE, F_CONTINUOUS, F_RECORD_CAND, F_ONE_SIDED = 1, 2, 4, 8, 16, 32
+F_REPTRI, F_THREADED, F_DISCRETE, F_CONTINUOUS, F_RECORD_CAND, F_ONE_SIDED, F_FLOAT = 1, 2, 4, 8, 16, 32, 64
 DEFAULT_FLAGS = F_REPTRI | F_THREADED | F_DISCRETE | F_CONTINUOUS
 
 

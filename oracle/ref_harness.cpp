@@ -60,13 +60,19 @@ struct State {
 };
 State g_state;
 
-enum { F_REPTRI = 1, F_THREADED = 2, F_DISCRETE = 4, F_CONTINUOUS = 8, F_RECORD_CAND = 16, F_ONE_SIDED = 32 };
+enum { F_REPTRI = 1, F_THREADED = 2, F_DISCRETE = 4, F_CONTINUOUS = 8, F_RECORD_CAND = 16, F_ONE_SIDED = 32, F_FLOAT = 64 };
 
-template <int DIM>
-int run(const double *V0, const double *V1, const int *P, int np, int pdim,
+// T = float runs the reference's BVHTree<float, DIM> on the coordinates
+// rounded to float (its own float arithmetic throughout).
+template <typename T, int DIM>
+int run(const double *V0d, const double *V1d, const int *P, int np, int pdim,
         double box_eta, double vf_eta, double ee_eta, int flags, const int *active)
 {
-    mcl::BVHTree<double, DIM> tree;
+    int nv = 0;
+    for (long long i = 0; i < (long long)np * pdim; ++i) nv = std::max(nv, P[i] + 1);
+    const std::vector<T> V0v(V0d, V0d + (size_t)nv * DIM), V1v(V1d, V1d + (size_t)nv * DIM);
+    const T *V0 = V0v.data(), *V1 = V1v.data();
+    mcl::BVHTree<T, DIM> tree;
     tree.options.box_eta = box_eta;
     tree.options.vf_ccd_eta = vf_eta;
     tree.options.ee_ccd_eta = ee_eta;
@@ -86,8 +92,8 @@ int run(const double *V0, const double *V1, const int *P, int np, int pdim,
             return false;
         };
     }
-    tree.append_pair = [&](const Eigen::Vector4i &s, bool is_vf, const double &toi) {
-        Hit h; for (int i = 0; i < 4; ++i) h.s[i] = s[i]; h.is_vf = is_vf; h.toi = toi;
+    tree.append_pair = [&](const Eigen::Vector4i &s, bool is_vf, const T &toi) {
+        Hit h; for (int i = 0; i < 4; ++i) h.s[i] = s[i]; h.is_vf = is_vf; h.toi = (double)toi;
         hits.push(h);
     };
     tree.append_discrete = [&](int p0, int p1) -> bool {
@@ -186,8 +192,13 @@ void ref_ctcd_vf(int dim, const double *V0, const double *V1, const int *sten, l
 int ref_run(int dim, const double *V0, const double *V1, const int *P, int np, int pdim,
             double box_eta, double vf_eta, double ee_eta, int flags, const int *active)
 {
-    if (dim == 3) return run<3>(V0, V1, P, np, pdim, box_eta, vf_eta, ee_eta, flags, active);
-    if (dim == 2) return run<2>(V0, V1, P, np, pdim, box_eta, vf_eta, ee_eta, flags, active);
+    if (flags & F_FLOAT) {
+        if (dim == 3) return run<float, 3>(V0, V1, P, np, pdim, box_eta, vf_eta, ee_eta, flags, active);
+        if (dim == 2) return run<float, 2>(V0, V1, P, np, pdim, box_eta, vf_eta, ee_eta, flags, active);
+        return -1;
+    }
+    if (dim == 3) return run<double, 3>(V0, V1, P, np, pdim, box_eta, vf_eta, ee_eta, flags, active);
+    if (dim == 2) return run<double, 2>(V0, V1, P, np, pdim, box_eta, vf_eta, ee_eta, flags, active);
     return -1;
 }
 

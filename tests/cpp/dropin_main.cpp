@@ -2,15 +2,53 @@
 // update(V0, V1, F) then traverse(V0, V1, F) with append_pair /
 // append_discrete collecting into vectors.  Scene in, results out, as raw
 // little-endian binaries (written / read by tests/test_cpp_dropin.py).
+// A third argument "float" runs mcl::BVHTree<float, 3> on the coordinates
+// rounded to float (toi written widened to double).
 #include "mclccd_b200/BVHTree.hpp"
 
 #include <cstdio>
 #include <cstdint>
 #include <vector>
 
+template <typename T>
+int run(const std::vector<double> &V0d, const std::vector<double> &V1d, const std::vector<int> &F, int np, double eta,
+        const char *out_path)
+{
+    const std::vector<T> V0(V0d.begin(), V0d.end()), V1(V1d.begin(), V1d.end());
+    mcl::BVHTree<T, 3> tree;
+    tree.options.box_eta = tree.options.vf_ccd_eta = tree.options.ee_ccd_eta = (T)eta;
+    std::vector<int> hs, ds;
+    std::vector<double> ht;
+    std::vector<unsigned char> hv;
+    tree.append_pair = [&](const mcl::Stencil &s, bool is_vf, const T &toi) {
+        for (int i = 0; i < 4; ++i) hs.push_back(s[i]);
+        hv.push_back(is_vf ? 1 : 0);
+        ht.push_back((double)toi);
+    };
+    tree.append_discrete = [&](int p0, int p1) { ds.push_back(p0); ds.push_back(p1); return false; };
+    try {
+        tree.update(V0.data(), V1.data(), F.data(), np, 3);
+        tree.traverse(V0.data(), V1.data(), F.data());
+    } catch (const mcl::CCDError &e) {
+        std::fprintf(stderr, "CCDError %d: %s\n", e.status, e.what());
+        return 1;
+    }
+    FILE *o = std::fopen(out_path, "wb");
+    if (!o) return 2;
+    int64_t n[2] = {(int64_t)hv.size(), (int64_t)ds.size() / 2};
+    std::fwrite(n, 8, 2, o);
+    std::fwrite(hs.data(), 4, hs.size(), o);
+    std::fwrite(hv.data(), 1, hv.size(), o);
+    std::fwrite(ht.data(), 8, ht.size(), o);
+    std::fwrite(ds.data(), 4, ds.size(), o);
+    std::fclose(o);
+    std::printf("hits %lld discrete %lld\n", (long long)n[0], (long long)n[1]);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
-    if (argc != 3) { std::fprintf(stderr, "usage: %s scene.bin out.bin\n", argv[0]); return 2; }
+    if (argc != 3 && argc != 4) { std::fprintf(stderr, "usage: %s scene.bin out.bin [float]\n", argv[0]); return 2; }
     FILE *f = std::fopen(argv[1], "rb");
     if (!f) return 2;
     int32_t hdr[3];   // nv, np, dim (== 3)
@@ -23,6 +61,7 @@ int main(int argc, char **argv)
         std::fread(F.data(), 4, F.size(), f) != F.size())
         return 2;
     std::fclose(f);
+    if (argc == 4) return run<float>(V0, V1, F, np, eta, argv[2]);
 
     mcl::BVHTree<double, 3> tree;
     tree.options.box_eta = tree.options.vf_ccd_eta = tree.options.ee_ccd_eta = eta;

@@ -49,3 +49,55 @@ def test_dropin_hooks_match_oracle(tmp_path):
     want = {(int(v),) + tuple(map(int, s)): float(t) for s, v, t in zip(p["hit_sten"], p["hit_is_vf"], p["hit_toi"])}
     assert got == want
     assert np.array_equal(sort_rows(ds), sort_rows(p["discrete"]))
+
+
+@pytest.mark.gpu
+def test_dropin_float_tree(tmp_path):
+    """mcl::BVHTree<float, 3>: the FP64 results for the float coordinates
+    (same sets; toi rounded down to float), compared with the reference's
+    own float instantiation run on the same float coordinates."""
+    from mclccd_b200 import scenes
+    from oracle.ref import DEFAULT_FLAGS, F_FLOAT, F_RECORD_CAND, Port, Reference, canonical_set, sort_rows
+    exe = build_demo(tmp_path)
+    V0, V1, F, eta = scenes.folded_cloth(40, seed=22)
+    scene = tmp_path / "scene.bin"
+    with open(scene, "wb") as f:
+        f.write(np.array([len(V0), len(F), 3], np.int32).tobytes())
+        f.write(np.array([eta], np.float64).tobytes())
+        f.write(V0.tobytes()); f.write(V1.tobytes()); f.write(F.astype(np.int32).tobytes())
+    out = tmp_path / "out.bin"
+    subprocess.run([exe, str(scene), str(out), "float"], check=True)
+    raw = out.read_bytes()
+    nh, nd = np.frombuffer(raw[:16], np.int64)
+    o = 16
+    hs = np.frombuffer(raw[o:o + 16 * nh], np.int32).reshape(-1, 4); o += 16 * nh
+    hv = np.frombuffer(raw[o:o + nh], np.uint8); o += nh
+    ht = np.frombuffer(raw[o:o + 8 * nh], np.float64); o += 8 * nh
+    ds = np.frombuffer(raw[o:o + 8 * nd], np.int32).reshape(-1, 2)
+    # the FP64 port on the float coordinates (and float eta), widened exactly
+    W0, W1 = V0.astype(np.float32).astype(np.float64), V1.astype(np.float32).astype(np.float64)
+    feta = float(np.float32(eta))
+    p = Port().run(W0, W1, F, feta)
+    assert np.array_equal(canonical_set(hs, hv), canonical_set(p["hit_sten"], p["hit_is_vf"]))
+    assert np.array_equal(sort_rows(ds), sort_rows(p["discrete"]))
+    want = {(int(v),) + tuple(map(int, s)): float(t) for s, v, t in zip(p["hit_sten"], p["hit_is_vf"], p["hit_toi"])}
+    got = {(int(v),) + tuple(map(int, s)): float(t) for s, v, t in zip(hs, hv, ht)}
+    for k, t in got.items():   # FP64 toi rounded down to float
+        w = want[k]
+        assert t <= w and float(np.float32(t)) == t
+        assert float(np.nextafter(np.float32(t), np.float32(np.inf))) > w   # compared in float64
+    # the reference's BVHTree<float, 3> (float arithmetic throughout)
+    r = Reference().run(V0, V1, F, eta, flags=DEFAULT_FLAGS | F_RECORD_CAND | F_FLOAT)
+    same = np.array_equal(canonical_set(hs, hv), canonical_set(r["hit_sten"], r["hit_is_vf"]))
+    def key(s, v):   # EE edge pairs in canonical order (the reference's follows its Kd-tree)
+        s = tuple(map(int, s))
+        if not v and min(s[0], s[1]) > min(s[2], s[3]):
+            s = s[2:] + s[:2]
+        return (int(v),) + s
+    rt = {key(s, v): float(t) for s, v, t in zip(r["hit_sten"], r["hit_is_vf"], r["hit_toi"])}
+    got = {key(s, v): t for (v, *s), t in got.items()}
+    common = set(rt) & set(got)
+    rel = max(abs(got[k] - rt[k]) / max(rt[k], 1e-30) for k in common)
+    print(f"float tree: {len(got)} hits; reference float instantiation {len(rt)} hits, same set {same}, "
+          f"max rel toi difference {rel:.2e}")
+    assert len(common) >= 0.999 * max(len(rt), len(got))

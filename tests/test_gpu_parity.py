@@ -261,3 +261,25 @@ def test_device_tensors(port):
     check_against_port(t, port, V0, V1, F, eta)
     t.traverse()   # NULL arrays: reuse the update's
     check_against_port(t, port, V0, V1, F, eta)
+
+
+def test_float32_coordinates():
+    # BVHTree<float, DIM>: float32 inputs (host arrays or CUDA tensors) give
+    # the FP64 results for the same coordinates widened exactly to double
+    torch = pytest.importorskip("torch")
+    for V0, V1, F, eta in (scenes.folded_cloth(32, seed=41), scenes.annulus_2d(256, seed=42)):
+        dim = V0.shape[1]
+        f0, f1 = V0.astype(np.float32), V1.astype(np.float32)
+        feta = float(np.float32(eta))
+        ref_t = run_gpu(f0.astype(np.float64), f1.astype(np.float64), F, feta)
+        want = hit_map(*ref_t.hits())
+        for a0, a1, aF in ((f0, f1, F), tuple(torch.from_numpy(x).cuda() for x in (f0, f1, F))):
+            t = BVHTree(dim)
+            t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = feta
+            t.update(a0, a1, aF)
+            t.traverse(a0, a1, aF)
+            assert hit_map(*t.hits()) == want
+            assert np.array_equal(sort_rows(t.discrete()), sort_rows(ref_t.discrete()))
+            t.update(a0, a1, aF)   # refit-only second step, traverse on the update's arrays
+            t.traverse()
+            assert hit_map(*t.hits()) == want
