@@ -284,6 +284,25 @@ typedef struct {
 } mclccd_tree_view;
 int mclccd_get_tree_view(const mclccd_tree *tree, mclccd_tree_view *view);
 
+/* Input forms other than row-major double (no counterpart in the
+ * reference; its Eigen overloads copy to RowMajor, BVHTree.hpp:151-186).
+ * One device pass converts them into the arrays the path runs on, so the
+ * caller's arrays are used as they are (host arrays are copied to the device
+ * unchanged, with no host-side conversion):
+ *   MCLCCD_IN_F32         V0/V1 are float (widened exactly to double);
+ *   MCLCCD_IN_V_COLMAJOR  V0/V1 column-major: coordinate k of vertex i at
+ *                         [k * nv + i] (Eigen's default MatrixXd layout);
+ *   MCLCCD_IN_P_COLMAJOR  P column-major: slot j of primitive i at
+ *                         [j * np + i] (Eigen's default MatrixXi layout).
+ * in_flags = 0 is mclccd_update / mclccd_traverse. */
+#define MCLCCD_IN_F32 1u
+#define MCLCCD_IN_V_COLMAJOR 2u
+#define MCLCCD_IN_P_COLMAJOR 4u
+int mclccd_update_ex(mclccd_tree *tree, const void *V0, const void *V1, int nv, const int *P, int np, int pdim,
+                     const int *active, int mem_kind, unsigned in_flags);
+int mclccd_traverse_ex(mclccd_tree *tree, const void *V0, const void *V1, int nv, const int *P, int mem_kind,
+                       unsigned in_flags);
+
 /* float coordinates (the reference's BVHTree<float, DIM> instantiations,
  * BVHTree.cpp:506-507): V0/V1 are float (nv x dim, mem_kind side) and are
  * widened exactly to double on the device, then update / traverse run as

@@ -128,16 +128,31 @@ public:
     }
 
 #ifdef MCLCCD_B200_HAVE_EIGEN
-    // Eigen convenience overloads (BVHTree.hpp:151-186): RowMajor copies, as
-    // the reference makes.
+    // Eigen overloads (BVHTree.hpp:151-186).  Where the reference makes
+    // RowMajor copies, matrices with contiguous storage in either order
+    // (e.g. the default column-major MatrixXd / MatrixXi) are passed as they
+    // are, with their layout, and converted on the device
+    // (mclccd_update_ex); other expressions are copied to RowMajor first.
     template <typename DerivedV, typename DerivedP>
     void update(const Eigen::MatrixBase<DerivedV> &V0, const Eigen::MatrixBase<DerivedV> &V1,
                 const Eigen::MatrixBase<DerivedP> &P, const Eigen::VectorXi &active = Eigen::VectorXi())
     {
         if (V0.rows() != V1.rows()) throw CCDError(MCLCCD_ERR_INVALID, "V0 and V1 row counts differ");
+        const int *act = active.size() == V0.rows() ? active.data() : nullptr;
+        unsigned f = 0;
+        if (direct_layout(V0, V1, P, f)) {
+            push_options();
+            const int rc = mclccd_update_ex(h_, V0.derived().data(), V1.derived().data(), (int)V0.rows(),
+                                            P.derived().data(), (int)P.rows(), (int)P.cols(), act, MCLCCD_MEM_HOST, f);
+            pull_options();
+            check(rc);
+            nv_ = (int)V0.rows();
+            np_ = (int)P.rows();
+            mem_ = MCLCCD_MEM_HOST;
+            return;
+        }
         RowV v0 = V0.template cast<T>(), v1 = V1.template cast<T>();
         RowP p = P.template cast<int>();
-        const int *act = active.size() == V0.rows() ? active.data() : nullptr;
         update(v0.data(), v1.data(), (int)v0.rows(), p.data(), (int)p.rows(), (int)p.cols(), act, MCLCCD_MEM_HOST);
     }
     template <typename DerivedV, typename DerivedP>
@@ -145,6 +160,15 @@ public:
                   const Eigen::MatrixBase<DerivedP> &P)
     {
         if (V0.rows() != V1.rows()) throw CCDError(MCLCCD_ERR_INVALID, "V0 and V1 row counts differ");
+        unsigned f = 0;
+        // a filter_pair without narrow_phase reads V0/V1 on the host as rows
+        if (!(filter_pair && !narrow_phase) && direct_layout(V0, V1, P, f)) {
+            push_options();
+            check(mclccd_traverse_ex(h_, V0.derived().data(), V1.derived().data(), (int)V0.rows(), P.derived().data(),
+                                     MCLCCD_MEM_HOST, f));
+            dispatch(nullptr, nullptr);
+            return;
+        }
         RowV v0 = V0.template cast<T>(), v1 = V1.template cast<T>();
         RowP p = P.template cast<int>();
         traverse(v0.data(), v1.data(), p.data());
@@ -179,6 +203,34 @@ private:
 #ifdef MCLCCD_B200_HAVE_EIGEN
     typedef Eigen::Matrix<T, Eigen::Dynamic, DIM, Eigen::RowMajor> RowV;
     typedef Eigen::Matrix<int, Eigen::Dynamic, Eigen::Dynamic, Eigen::RowMajor> RowP;
+
+    // 0: contiguous rows, 1: contiguous columns, -1: neither.
+    template <typename D>
+    static int layout_of(const Eigen::MatrixBase<D> &m)
+    {
+        const D &d = m.derived();
+        if (d.innerStride() != 1) return -1;
+        if (D::IsRowMajor) return d.outerStride() == d.cols() ? 0 : -1;
+        return d.outerStride() == d.rows() ? 1 : -1;
+    }
+    // Whether V0, V1 (scalar T, DIM columns, same layout) and P (int) can be
+    // passed as they are; f receives the mclccd_update_ex input flags.
+    template <typename DV, typename DP>
+    static bool direct_layout(const Eigen::MatrixBase<DV> &V0, const Eigen::MatrixBase<DV> &V1,
+                              const Eigen::MatrixBase<DP> &P, unsigned &f)
+    {
+        if constexpr (std::is_same<typename DV::Scalar, T>::value && std::is_same<typename DP::Scalar, int>::value &&
+                      (int(DV::Flags) & Eigen::DirectAccessBit) != 0 && (int(DP::Flags) & Eigen::DirectAccessBit) != 0) {
+            const int l0 = layout_of(V0), l1 = layout_of(V1), lp = layout_of(P);
+            if (V0.cols() != DIM || V1.cols() != DIM || l0 < 0 || l0 != l1 || lp < 0) return false;
+            f = (kFloat ? MCLCCD_IN_F32 : 0u) | (l0 == 1 ? MCLCCD_IN_V_COLMAJOR : 0u) |
+                (lp == 1 ? MCLCCD_IN_P_COLMAJOR : 0u);
+            return true;
+        } else {
+            (void)V0; (void)V1; (void)P; (void)f;
+            return false;
+        }
+    }
 #endif
     mclccd_tree *h_ = nullptr;
     int nv_ = 0, np_ = 0, mem_ = MCLCCD_MEM_HOST;

@@ -64,6 +64,8 @@ def lib():
         "mclccd_update": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int], C.c_int),
         "mclccd_traverse": ([vp, vp, vp, C.c_int, vp, C.c_int], C.c_int),
         "mclccd_update_f32": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int], C.c_int),
+        "mclccd_update_ex": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int, C.c_uint], C.c_int),
+        "mclccd_traverse_ex": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_uint], C.c_int),
         "mclccd_traverse_f32": ([vp, vp, vp, C.c_int, vp, C.c_int], C.c_int),
         "mclccd_counts": ([vp, llp, llp, llp, llp, llp], C.c_int),
         "mclccd_get_hits": ([vp, C.c_int, C.c_longlong, vp, vp, vp], C.c_int),
@@ -105,6 +107,30 @@ def _is_f32(a):
         import torch
         return a.dtype == torch.float32
     return getattr(a, "dtype", None) == np.float32
+
+
+IN_F32, IN_V_COLMAJOR, IN_P_COLMAJOR = 1, 2, 4
+
+
+def _colmajor(a, dtype):
+    """True for a 2D column-major (Fortran-order) array of dtype: passed to
+    the library as it is, with the layout flag, instead of a row-major copy."""
+    if a is None:
+        return False
+    if _is_torch_cuda(a):
+        import torch
+        tdt = {np.float64: torch.float64, np.float32: torch.float32, np.int32: torch.int32}[dtype]
+        return (a.dim() == 2 and a.dtype == tdt and a.shape[0] > 1 and a.shape[1] > 1
+                and a.stride() == (1, a.shape[0]))
+    return (isinstance(a, np.ndarray) and a.ndim == 2 and a.dtype == dtype and a.shape[0] > 1 and a.shape[1] > 1
+            and a.flags.f_contiguous and not a.flags.c_contiguous)
+
+
+def _arg_colmajor(a):
+    """(pointer, mem_kind, keepalive, rows) of a column-major array."""
+    if _is_torch_cuda(a):
+        return C.c_void_p(a.data_ptr()), MEM_DEVICE, a, a.shape[0]
+    return C.c_void_p(a.ctypes.data), MEM_HOST, a, a.shape[0]
 
 
 def _arg(a, dtype, cols=None):
@@ -227,9 +253,11 @@ class BVHTree:
         double on the device)."""
         f32 = _is_f32(V0)
         vt = np.float32 if f32 else np.float64
-        pv0, k0, a0, nv = _arg(V0, vt, self.dim)
-        pv1, k1, a1, nv1 = _arg(V1, vt, self.dim)
-        pp, kp, ap, npr = _arg(P, np.int32)
+        vcol = _colmajor(V0, vt) and _colmajor(V1, vt)
+        pcol = _colmajor(P, np.int32)
+        pv0, k0, a0, nv = _arg_colmajor(V0) if vcol else _arg(V0, vt, self.dim)
+        pv1, k1, a1, nv1 = _arg_colmajor(V1) if vcol else _arg(V1, vt, self.dim)
+        pp, kp, ap, npr = _arg_colmajor(P) if pcol else _arg(P, np.int32)
         pa, ka, aa, _ = _arg(active, np.int32)
         if nv != nv1:   # BVHTree.hpp:160: silently ignored by the reference
             raise ValueError("V0 and V1 must have the same number of rows")
@@ -237,9 +265,10 @@ class BVHTree:
         if len(kinds) > 1:
             raise ValueError("V0, V1, P and active must all be host arrays or all CUDA tensors")
         pdim = ap.shape[1] if ap.ndim == 2 else self.dim
+        flags = (IN_F32 if f32 else 0) | (IN_V_COLMAJOR if vcol else 0) | (IN_P_COLMAJOR if pcol else 0)
         self._push_options()
-        upd = self._L.mclccd_update_f32 if f32 else self._L.mclccd_update
-        rc = upd(self._h, pv0, pv1, nv, pp, npr, pdim, pa, kinds.pop() if kinds else MEM_HOST)
+        rc = self._L.mclccd_update_ex(self._h, pv0, pv1, nv, pp, npr, pdim, pa, kinds.pop() if kinds else MEM_HOST,
+                                      flags)
         self._pull_options()
         self._check(rc, self._h)
         self._keep = [a0, a1, ap, aa]
@@ -249,13 +278,15 @@ class BVHTree:
         """BVHTree::traverse (BVHTree.cpp:129-159), then the hooks."""
         f32 = _is_f32(V0)
         vt = np.float32 if f32 else np.float64
-        pv0, k0, a0, nv = _arg(V0, vt, self.dim)
-        pv1, k1, a1, _ = _arg(V1, vt, self.dim)
-        pp, kp, ap, _ = _arg(P, np.int32)
+        vcol = _colmajor(V0, vt) and _colmajor(V1, vt)
+        pcol = _colmajor(P, np.int32)
+        pv0, k0, a0, nv = _arg_colmajor(V0) if vcol else _arg(V0, vt, self.dim)
+        pv1, k1, a1, _ = _arg_colmajor(V1) if vcol else _arg(V1, vt, self.dim)
+        pp, kp, ap, _ = _arg_colmajor(P) if pcol else _arg(P, np.int32)
         kind = k0 if k0 is not None else MEM_HOST
+        flags = (IN_F32 if f32 else 0) | (IN_V_COLMAJOR if vcol else 0) | (IN_P_COLMAJOR if pcol else 0)
         self._push_options()
-        trv = self._L.mclccd_traverse_f32 if f32 else self._L.mclccd_traverse
-        self._check(trv(self._h, pv0, pv1, nv, pp, kind), self._h)
+        self._check(self._L.mclccd_traverse_ex(self._h, pv0, pv1, nv, pp, kind, flags), self._h)
         if V0 is not None:
             self._nv = nv
         self._dispatch(V0, V1)

@@ -58,13 +58,13 @@ struct mclccd_tree {
     DevBuf cent, bounds, keys, vals, keys_alt, vals_alt, sort_scratch;
     DevBuf nodes, leaf_parent, visits, leaf_box, leaf_active;
     DevBuf pairs, vf, ee, hit_sten, hit_toi, hit_isvf, disc, counters, diff, fp64_queue;
-    DevBuf f32_V, f32_P, f32_act;   // float-input staging (mclccd_update_f32 / mclccd_traverse_f32)
+    DevBuf in_V, in_P, in_act, in_tmp;   // input conversion staging (mclccd_update_ex / mclccd_traverse_ex)
     std::vector<DevBuf *> all()
     {
         return {&V0d, &V1d, &Pd, &Pstage, &actd, &pflags, &pflags_tmp, &vowner, &ekeys, &eowner, &cent, &bounds,
                 &keys, &vals, &keys_alt, &vals_alt, &sort_scratch, &nodes, &leaf_parent, &visits, &leaf_box,
                 &leaf_active, &pairs, &vf, &ee, &hit_sten, &hit_toi, &hit_isvf, &disc, &counters, &diff,
-                &fp64_queue, &f32_V, &f32_P, &f32_act};
+                &fp64_queue, &in_V, &in_P, &in_act, &in_tmp};
     }
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
@@ -128,6 +128,86 @@ int device_errors(mclccd_tree *t, unsigned err)
 }
 
 } // namespace
+
+// Inputs in other forms than row-major double (float coordinates, column-
+// major V or P): one pass converts them on the device into the row-major
+// double / int arrays the path runs on.  Widening float -> double is exact.
+template <typename T, bool COL>
+__global__ void k_stage_positions(const T *__restrict__ a, const T *__restrict__ b, double *__restrict__ oa,
+                                  double *__restrict__ ob, int nv, int dim)
+{
+    const long long n = (long long)nv * dim;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+        const long long d = COL ? (s % nv) * dim + s / nv : s;   // source index s -> row-major index d
+        oa[d] = (double)a[s];
+        ob[d] = (double)b[s];
+    }
+}
+
+__global__ void k_stage_prims(const int *__restrict__ P, int *__restrict__ out, int np, int pdim)
+{
+    const long long n = (long long)np * pdim;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x)
+        out[(s % np) * pdim + s / np] = P[s];
+}
+
+static int stage_grid(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 16)); }
+
+// V0/V1 (in_flags form, mem_kind side) -> t->V0d/V1d (row-major double, device).
+static int stage_positions(mclccd_tree *t, const void *V0, const void *V1, int nv, int mem_kind, unsigned in_flags)
+{
+    const int dim = t->dim;
+    const long long n = (long long)nv * dim;
+    const size_t esz = (in_flags & MCLCCD_IN_F32) ? sizeof(float) : sizeof(double);
+    cudaStream_t st = t->stream;
+    MC_CUDA(t, ensure(t->V0d, sizeof(double) * (size_t)n));
+    MC_CUDA(t, ensure(t->V1d, sizeof(double) * (size_t)n));
+    const void *a = V0, *b = V1;
+    if (mem_kind == MCLCCD_MEM_HOST) {
+        MC_CUDA(t, ensure(t->in_V, 2 * esz * (size_t)n));
+        char *s = static_cast<char *>(t->in_V.p);
+        MC_CUDA(t, cudaMemcpyAsync(s, V0, esz * (size_t)n, cudaMemcpyHostToDevice, st));
+        MC_CUDA(t, cudaMemcpyAsync(s + esz * n, V1, esz * (size_t)n, cudaMemcpyHostToDevice, st));
+        a = s;
+        b = s + esz * n;
+    }
+    const bool col = (in_flags & MCLCCD_IN_V_COLMAJOR) != 0;
+    double *oa = as<double>(t->V0d), *ob = as<double>(t->V1d);
+    const int g = stage_grid(n);
+    if (in_flags & MCLCCD_IN_F32) {
+        if (col) k_stage_positions<float, true><<<g, 256, 0, st>>>((const float *)a, (const float *)b, oa, ob, nv, dim);
+        else k_stage_positions<float, false><<<g, 256, 0, st>>>((const float *)a, (const float *)b, oa, ob, nv, dim);
+    } else {
+        k_stage_positions<double, true><<<g, 256, 0, st>>>((const double *)a, (const double *)b, oa, ob, nv, dim);
+    }
+    ++t->launches;
+    MC_CUDA(t, cudaGetLastError());
+    return MCLCCD_OK;
+}
+
+// An int array on the mem_kind side -> a device pointer; column-major P
+// (slot j of primitive i at [j * np + i]) is transposed to row-major.
+static int stage_ints(mclccd_tree *t, DevBuf &buf, DevBuf &tmp, const int *src, int rows, int cols, bool colmajor,
+                      int mem_kind, const int *&out)
+{
+    out = src;
+    if (!src) return MCLCCD_OK;
+    const size_t count = (size_t)rows * cols;
+    if (mem_kind == MCLCCD_MEM_HOST) {
+        DevBuf &dst = colmajor ? tmp : buf;
+        MC_CUDA(t, ensure(dst, sizeof(int) * std::max<size_t>(count, 1)));
+        MC_CUDA(t, cudaMemcpyAsync(dst.p, src, sizeof(int) * count, cudaMemcpyHostToDevice, t->stream));
+        out = as<int>(dst);
+    }
+    if (colmajor) {
+        MC_CUDA(t, ensure(buf, sizeof(int) * std::max<size_t>(count, 1)));
+        k_stage_prims<<<stage_grid((long long)count), 256, 0, t->stream>>>(out, as<int>(buf), rows, cols);
+        ++t->launches;
+        MC_CUDA(t, cudaGetLastError());
+        out = as<int>(buf);
+    }
+    return MCLCCD_OK;
+}
 
 extern "C" {
 
@@ -358,54 +438,14 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
     return MCLCCD_OK;
 }
 
-// float inputs: exact widening to the FP64 arrays the path runs on.
-__global__ void k_widen(const float *__restrict__ a, const float *__restrict__ b, double *__restrict__ oa,
-                        double *__restrict__ ob, long long n)
-{
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        oa[i] = (double)a[i];
-        ob[i] = (double)b[i];
-    }
-}
-
-// V0/V1 (float, mem_kind side) -> t->V0d/V1d (double, device).
-static int widen_positions(mclccd_tree *t, const float *V0, const float *V1, int nv, int mem_kind)
-{
-    const long long n = (long long)nv * t->dim;
-    cudaStream_t st = t->stream;
-    MC_CUDA(t, ensure(t->V0d, sizeof(double) * (size_t)n));
-    MC_CUDA(t, ensure(t->V1d, sizeof(double) * (size_t)n));
-    const float *a = V0, *b = V1;
-    if (mem_kind == MCLCCD_MEM_HOST) {
-        MC_CUDA(t, ensure(t->f32_V, 2 * sizeof(float) * (size_t)n));
-        float *s = as<float>(t->f32_V);
-        MC_CUDA(t, cudaMemcpyAsync(s, V0, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st));
-        MC_CUDA(t, cudaMemcpyAsync(s + n, V1, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st));
-        a = s;
-        b = s + n;
-    }
-    const long long g = std::min<long long>((n + 255) / 256, 148 * 16);
-    k_widen<<<(int)std::max<long long>(g, 1), 256, 0, st>>>(a, b, as<double>(t->V0d), as<double>(t->V1d), n);
-    ++t->launches;
-    MC_CUDA(t, cudaGetLastError());
-    return MCLCCD_OK;
-}
-
-// An int array on the mem_kind side -> a device pointer (staged when host).
-static int stage_ints(mclccd_tree *t, DevBuf &buf, const int *src, size_t count, int mem_kind, const int *&out)
-{
-    out = src;
-    if (!src || mem_kind != MCLCCD_MEM_HOST) return MCLCCD_OK;
-    MC_CUDA(t, ensure(buf, sizeof(int) * std::max<size_t>(count, 1)));
-    MC_CUDA(t, cudaMemcpyAsync(buf.p, src, sizeof(int) * count, cudaMemcpyHostToDevice, t->stream));
-    out = as<int>(buf);
-    return MCLCCD_OK;
-}
-
-int mclccd_update_f32(mclccd_tree *t, const float *V0, const float *V1, int nv, const int *P, int np, int pdim,
-                      const int *active, int mem_kind)
+int mclccd_update_ex(mclccd_tree *t, const void *V0, const void *V1, int nv, const int *P, int np, int pdim,
+                     const int *active, int mem_kind, unsigned in_flags)
 {
     if (!t) return MCLCCD_ERR_INVALID;
+    if (in_flags & ~(MCLCCD_IN_F32 | MCLCCD_IN_V_COLMAJOR | MCLCCD_IN_P_COLMAJOR))
+        return fail(t, MCLCCD_ERR_INVALID, "unknown input flags");
+    if (in_flags == 0)
+        return mclccd_update(t, (const double *)V0, (const double *)V1, nv, P, np, pdim, active, mem_kind);
     t->err.clear();
     if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
     if (np < 0 || nv < 0) return fail(t, MCLCCD_ERR_INVALID, "negative size");
@@ -414,28 +454,69 @@ int mclccd_update_f32(mclccd_tree *t, const float *V0, const float *V1, int nv, 
     if (pdim < 1 || pdim > 4) return fail(t, MCLCCD_ERR_INVALID, "pdim must be in [1, 4]");
     DeviceGuard g(t->device);
     const int *dP = nullptr, *dact = nullptr;
-    if (int rc = widen_positions(t, V0, V1, nv, mem_kind)) return rc;
-    if (int rc = stage_ints(t, t->f32_P, P, (size_t)np * pdim, mem_kind, dP)) return rc;
-    if (int rc = stage_ints(t, t->f32_act, active, (size_t)nv, mem_kind, dact)) return rc;
-    return mclccd_update(t, as<double>(t->V0d), as<double>(t->V1d), nv, dP, np, pdim, dact, MCLCCD_MEM_DEVICE);
+    const bool pcol = (in_flags & MCLCCD_IN_P_COLMAJOR) != 0;
+    if (in_flags & (MCLCCD_IN_F32 | MCLCCD_IN_V_COLMAJOR)) {
+        if (int rc = stage_positions(t, V0, V1, nv, mem_kind, in_flags)) return rc;
+    } else if (mem_kind == MCLCCD_MEM_HOST) {   // row-major double on the host: plain copies
+        const size_t vb = sizeof(double) * (size_t)nv * t->dim;
+        MC_CUDA(t, ensure(t->V0d, vb));
+        MC_CUDA(t, ensure(t->V1d, vb));
+        MC_CUDA(t, cudaMemcpyAsync(t->V0d.p, V0, vb, cudaMemcpyHostToDevice, t->stream));
+        MC_CUDA(t, cudaMemcpyAsync(t->V1d.p, V1, vb, cudaMemcpyHostToDevice, t->stream));
+    }
+    const bool vdev = !(in_flags & (MCLCCD_IN_F32 | MCLCCD_IN_V_COLMAJOR)) && mem_kind == MCLCCD_MEM_DEVICE;
+    if (int rc = stage_ints(t, t->in_P, t->in_tmp, P, np, pdim, pcol, mem_kind, dP)) return rc;
+    if (int rc = stage_ints(t, t->in_act, t->in_tmp, active, nv, 1, false, mem_kind, dact)) return rc;
+    const double *a = vdev ? (const double *)V0 : as<double>(t->V0d), *b = vdev ? (const double *)V1 : as<double>(t->V1d);
+    return mclccd_update(t, a, b, nv, dP, np, pdim, dact, MCLCCD_MEM_DEVICE);
 }
 
-int mclccd_traverse_f32(mclccd_tree *t, const float *V0, const float *V1, int nv, const int *P, int mem_kind)
+int mclccd_traverse_ex(mclccd_tree *t, const void *V0, const void *V1, int nv, const int *P, int mem_kind,
+                       unsigned in_flags)
 {
     if (!t) return MCLCCD_ERR_INVALID;
+    if (in_flags & ~(MCLCCD_IN_F32 | MCLCCD_IN_V_COLMAJOR | MCLCCD_IN_P_COLMAJOR))
+        return fail(t, MCLCCD_ERR_INVALID, "unknown input flags");
+    if (in_flags == 0 || (!V0 && !V1 && !P))
+        return mclccd_traverse(t, (const double *)V0, (const double *)V1, nv, P, mem_kind);
     t->err.clear();
-    if (!V0 && !V1 && !P) return mclccd_traverse(t, nullptr, nullptr, 0, nullptr, MCLCCD_MEM_DEVICE);
     if (!V0 || !V1 || !P) return fail(t, MCLCCD_ERR_INVALID, "V0, V1, P must all be given (or all NULL)");
     if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
     if (!t->built) return fail(t, MCLCCD_ERR_STATE, "traverse before a successful update");
     if (nv <= 0) nv = t->nv;
     DeviceGuard g(t->device);
     const int *dP = nullptr;
-    if (int rc = widen_positions(t, V0, V1, nv, mem_kind)) return rc;
-    if (int rc = stage_ints(t, t->f32_P, P, (size_t)t->np * t->dim, mem_kind, dP)) return rc;
-    t->upd_V0 = as<double>(t->V0d);   // the update's arrays were overwritten
-    t->upd_V1 = as<double>(t->V1d);
-    return mclccd_traverse(t, as<double>(t->V0d), as<double>(t->V1d), nv, dP, MCLCCD_MEM_DEVICE);
+    const bool vconv = (in_flags & (MCLCCD_IN_F32 | MCLCCD_IN_V_COLMAJOR)) != 0;
+    if (vconv) {
+        if (int rc = stage_positions(t, V0, V1, nv, mem_kind, in_flags)) return rc;
+    } else if (mem_kind == MCLCCD_MEM_HOST) {
+        const size_t vb = sizeof(double) * (size_t)nv * t->dim;
+        MC_CUDA(t, ensure(t->V0d, vb));
+        MC_CUDA(t, ensure(t->V1d, vb));
+        MC_CUDA(t, cudaMemcpyAsync(t->V0d.p, V0, vb, cudaMemcpyHostToDevice, t->stream));
+        MC_CUDA(t, cudaMemcpyAsync(t->V1d.p, V1, vb, cudaMemcpyHostToDevice, t->stream));
+    }
+    if (int rc = stage_ints(t, t->in_P, t->in_tmp, P, t->np, t->dim, (in_flags & MCLCCD_IN_P_COLMAJOR) != 0,
+                            mem_kind, dP))
+        return rc;
+    const bool vdev = !vconv && mem_kind == MCLCCD_MEM_DEVICE;
+    const double *a = vdev ? (const double *)V0 : as<double>(t->V0d), *b = vdev ? (const double *)V1 : as<double>(t->V1d);
+    if (!vdev) {   // the update's arrays were overwritten
+        t->upd_V0 = a;
+        t->upd_V1 = b;
+    }
+    return mclccd_traverse(t, a, b, nv, dP, MCLCCD_MEM_DEVICE);
+}
+
+int mclccd_update_f32(mclccd_tree *t, const float *V0, const float *V1, int nv, const int *P, int np, int pdim,
+                      const int *active, int mem_kind)
+{
+    return mclccd_update_ex(t, V0, V1, nv, P, np, pdim, active, mem_kind, MCLCCD_IN_F32);
+}
+
+int mclccd_traverse_f32(mclccd_tree *t, const float *V0, const float *V1, int nv, const int *P, int mem_kind)
+{
+    return mclccd_traverse_ex(t, V0, V1, nv, P, mem_kind, MCLCCD_IN_F32);
 }
 
 int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, const int *P, int mem_kind)
