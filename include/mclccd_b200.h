@@ -325,13 +325,18 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
  * tree-walk form (1: warp-cooperative packets, 0: one query per thread) and
  * the FP64 ACCD form (1: stencils that go on after the first distance are
  * re-binned in shared memory so warps run heads or tails, never both; 0, the
- * default and faster on B200: one stencil per thread start to end).  Results
- * do not depend on any of them. */
+ * default and faster on B200: one stencil per thread start to end), and the
+ * walk's Morton window (W = 8, 16 (default), 32, 64 or 128: each query
+ * first tests the W leaves after it in Morton order, staged by its block in
+ * shared memory, then walks the tree only for leaves beyond them; 0: tree
+ * walk only).
+ * Results do not depend on any of them. */
 #define MCLCCD_TUNE_EXPAND_GRID 0
 #define MCLCCD_TUNE_ACCD_GRID 1
 #define MCLCCD_TUNE_WALK_PACKET 2
 #define MCLCCD_TUNE_ACCD_REBIN 3
-#define MCLCCD_TUNE_COUNT 4
+#define MCLCCD_TUNE_WALK_WINDOW 4
+#define MCLCCD_TUNE_COUNT 5
 int mclccd_set_tuning(mclccd_tree *tree, int key, int value);
 int mclccd_get_tuning(const mclccd_tree *tree, int key, int *value);
 

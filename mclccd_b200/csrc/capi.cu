@@ -69,7 +69,7 @@ struct mclccd_tree {
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
     cudaEvent_t ev[8] = {};
-    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0};
+    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16};
 };
 
 namespace {
@@ -590,7 +590,8 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
         const bool certified = t->precision == MCLCCD_PREC_FP32_CERTIFIED;
         if (certified && cont) MC_CUDA(t, ensure(t->fp64_queue, sizeof(unsigned) * std::max(t->cap_vf, t->cap_ee)));
         MC_CUDA(t, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
-        launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], as<Node>(t->nodes), t->leaf_box.p,
+        launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes),
+                        t->leaf_box.p,
                         as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
                         cnt, st);
         if (prof) cudaEventRecord(t->ev[4], st);
@@ -997,7 +998,10 @@ int mclccd_set_tuning(mclccd_tree *t, int key, int value)
 {
     if (!t || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
     const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_ACCD_REBIN;
-    if (flag ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))
+    if (key == MCLCCD_TUNE_WALK_WINDOW) {
+        if (value != 0 && value != 8 && value != 16 && value != 32 && value != 64 && value != 128)
+            return fail(t, MCLCCD_ERR_INVALID, "walk window must be 0, 8, 16, 32, 64 or 128");
+    } else if (flag ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))
         return fail(t, MCLCCD_ERR_INVALID, "tuning value out of range");
     t->tune[key] = value;
     return MCLCCD_OK;

@@ -25,7 +25,7 @@ void launch_sort_pairs(unsigned *keys, int *vals, unsigned *keys_alt, int *vals_
                        void *scratch, Counters *cnt, cudaStream_t st);
 
 // traverse.cu
-void launch_traverse(int dim, int packet, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
+void launch_traverse(int dim, int packet, int window, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
                      const int *sorted, int n, int2 *pairs, unsigned long long cap, Counters *cnt, cudaStream_t st);
 void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,
                          const unsigned char *flags, const double *V1, int nv, int4 *vf, unsigned long long vf_cap,

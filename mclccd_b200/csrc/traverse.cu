@@ -109,6 +109,116 @@ k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf
 // Control flow is warp-uniform (one stack per warp, in shared memory); each
 // lane still applies exactly its own tests, so the pairs found are the same.
 // ---------------------------------------------------------------------------
+// Window form (MCLCCD_TUNE_WALK_WINDOW = W).  Most of a query's overlapping
+// leaves are close to it in Morton order, where the tree walk is also most
+// divergent.  So each block first stages the FP32 boxes (rounded outward) and
+// active flags of the leaves after its 128 queries, (q0, q0 + 127 + W], in
+// shared memory with coalesced loads; each query tests the W leaves after it
+// from there, all lanes in step; then it walks the tree only into subtrees
+// that hold leaves beyond q + W.  Every leaf k > q is tested exactly once, by
+// the same three-valued FP32 test with the FP64 fallback, so the leaf-pair
+// set is the one of k_traverse.
+// 4 resident blocks per SM: the staged window and the walk state need 128
+// registers to run without spills (at 96 the spills in the walk loop cost
+// more than the window saves).
+template <int DIM, int W>
+__global__ void __launch_bounds__(128, 4)
+k_traverse_window(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
+                  const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
+                  int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
+{
+    constexpr int S = DIM == 3 ? 3 : 2;
+    constexpr int NB = 127 + W;
+    __shared__ float s_box[NB][4 * DIM];   // t0lo, t0hi, t1lo, t1hi
+    __shared__ unsigned char s_act[NB];
+    __shared__ int stack[kStackDepth][128];
+    const int tid = threadIdx.x;
+    const int q0 = blockIdx.x * 128;
+    if (q0 >= n - 1) return;   // whole block past the end
+    for (int i = tid; i < NB; i += 128) {
+        const int k = q0 + 1 + i;
+        if (k < n) {
+            const LeafBox<DIM> &kb = leaf_box[k];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                s_box[i][d] = __double2float_rd(kb.lo0[d]);
+                s_box[i][DIM + d] = __double2float_ru(kb.hi0[d]);
+                s_box[i][2 * DIM + d] = __double2float_rd(kb.lo1[d]);
+                s_box[i][3 * DIM + d] = __double2float_ru(kb.hi1[d]);
+            }
+            s_act[i] = leaf_active[k];
+        }
+    }
+    __syncthreads();
+    const int q = q0 + tid;
+    if (q >= n - 1) return;
+    const bool qact = leaf_active[q] != 0;
+    const int qprim = sorted[q];
+    Box2T<DIM> qbox;
+    {
+        const LeafBox<DIM> &qb = leaf_box[q];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            qbox.t0lo[k] = __double2float_rd(qb.lo0[k]); qbox.t0hi[k] = __double2float_ru(qb.hi0[k]);
+            qbox.t1lo[k] = __double2float_rd(qb.lo1[k]); qbox.t1hi[k] = __double2float_ru(qb.hi1[k]);
+        }
+    }
+    auto leaf = [&](int k, const Box2T<DIM> &kbox) {
+        int r = leaf_test3<DIM>(qbox, inner<DIM>(qbox), kbox);
+        if (r == 2) r = leaf_boxes_intersect<DIM>(leaf_box[q], leaf_box[k]) ? 1 : 0;
+        if (r == 1) {
+            const int kprim = __ldg(sorted + k);
+            unsigned long long slot = warp_append(&cnt->n_pairs);
+            if (slot < cap) pairs[slot] = make_int2(min(qprim, kprim), max(qprim, kprim));
+        }
+    };
+    // 1. the window: leaves q + 1 .. q + W from shared memory
+    const int qw = min(q + W, n - 1);
+    for (int k = q + 1; k <= qw; ++k) {
+        const int i = k - q0 - 1;
+        if (!(qact || s_act[i])) continue;
+        Box2T<DIM> kb;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            kb.t0lo[d] = s_box[i][d]; kb.t0hi[d] = s_box[i][DIM + d];
+            kb.t1lo[d] = s_box[i][2 * DIM + d]; kb.t1hi[d] = s_box[i][3 * DIM + d];
+        }
+        leaf(k, kb);
+    }
+    // 2. the tree, for leaves beyond the window
+    int sp = 0, node = 0;
+    for (int steps = 0;; ++steps) {
+        if (steps >= n) { atomicOr(&cnt->err, kErrStack); break; }
+        float4 ls[S], rs[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) { ls[i] = __ldg(&nodes[node].l[i]); rs[i] = __ldg(&nodes[node].r[i]); }
+        const int4 d = __ldg(&nodes[node].d);
+        const int split = d.x, meta = d.y, last = d.z;
+        Box2T<DIM> lb, rb;
+        unpack_child<DIM>(ls, lb);
+        unpack_child<DIM>(rs, rb);
+        const bool lact = ((meta >> 8) & 0xff) != 0, ract = ((meta >> 16) & 0xff) != 0;
+        bool lok = split > qw && (qact || lact);
+        bool rok = last > qw && (qact || ract);
+        if (lok && (meta & kMetaLeftLeaf)) { leaf(split, lb); lok = false; }
+        if (rok && (meta & kMetaRightLeaf)) { leaf(split + 1, rb); rok = false; }
+        lok = lok && boxes_may_intersect<DIM>(qbox, lb);
+        rok = rok && boxes_may_intersect<DIM>(qbox, rb);
+        if (lok) {
+            if (rok) {
+                if (sp < kStackDepth) stack[sp++][tid] = split + 1;
+                else atomicOr(&cnt->err, kErrStack);
+            }
+            node = split;
+        } else if (rok) {
+            node = split + 1;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp][tid];
+        }
+    }
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(128)
 k_traverse_packet(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
@@ -267,13 +377,31 @@ k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, cons
     }
 }
 
-void launch_traverse(int dim, int packet, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
-                     const int *sorted, int n, int2 *pairs, unsigned long long cap, Counters *cnt, cudaStream_t st)
+void launch_traverse(int dim, int packet, int window, const Node *nodes, const void *leaf_box,
+                     const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs, unsigned long long cap,
+                     Counters *cnt, cudaStream_t st)
 {
     if (n < 2) return;
     const int g = (n - 1 + 127) / 128;
     const auto *lb3 = reinterpret_cast<const LeafBox<3> *>(leaf_box);
     const auto *lb2 = reinterpret_cast<const LeafBox<2> *>(leaf_box);
+    if (window) {
+#define MCLCCD_WINDOW_CASE(Wv)                                                                                     \
+    case Wv:                                                                                                       \
+        cudaFuncSetAttribute(k_traverse_window<3, Wv>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);        \
+        cudaFuncSetAttribute(k_traverse_window<2, Wv>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);        \
+        if (dim == 3) k_traverse_window<3, Wv><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, pairs, cap, cnt); \
+        else k_traverse_window<2, Wv><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, pairs, cap, cnt);         \
+        return;
+        switch (window) {
+            MCLCCD_WINDOW_CASE(8)
+            MCLCCD_WINDOW_CASE(16)
+            MCLCCD_WINDOW_CASE(32)
+            MCLCCD_WINDOW_CASE(64)
+            MCLCCD_WINDOW_CASE(128)
+        }
+#undef MCLCCD_WINDOW_CASE
+    }
     if (packet) {
         if (dim == 3) k_traverse_packet<3><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, pairs, cap, cnt);
         else k_traverse_packet<2><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, pairs, cap, cnt);

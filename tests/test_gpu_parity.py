@@ -87,6 +87,28 @@ def test_cfg0_folded_cloth(port):
     check_against_port(t, port, V0, V1, F, eta)
 
 
+@pytest.mark.parametrize("window", [32, 128])
+@pytest.mark.parametrize("scene", ["wavy", "annulus", "active"])
+def test_walk_window_against_port(port, window, scene):
+    # the Morton-window walk (shared-memory scan of the next W leaves, then
+    # the tree beyond them) finds exactly the reference's leaf pairs
+    V0, V1, F, eta = scenes.wavy_cloth(1025, rows=97, seed=5) if scene != "annulus" else scenes.annulus_2d(500, seed=6)
+    t = BVHTree(V0.shape[1])
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.set_tuning(walk_window=window)
+    if scene == "active":   # partial-mesh CCD: only a band of vertices active
+        act = (np.arange(len(V0)) % 7 < 2).astype(np.int32)
+        t.update(V0, V1, F, active=act)
+        t.traverse(V0, V1, F)
+        p = port.run(V0, V1, F, eta, active=act)
+        cs, cv = t.candidates()
+        assert np.array_equal(canonical_set(cs, cv), canonical_set(p["cand_sten"], p["cand_is_vf"]))
+        return
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    check_against_port(t, port, V0, V1, F, eta)
+
+
 @pytest.mark.parametrize("dim", [3, 2])
 def test_rebinned_accd_against_port(port, dim):
     # the re-binned ACCD form (heads and tails in separate warp passes) gives
