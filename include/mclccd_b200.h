@@ -329,14 +329,17 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
  * walk's Morton window (W = 8, 16 (default), 32, 64 or 128: each query
  * first tests the W leaves after it in Morton order, staged by its block in
  * shared memory, then walks the tree only for leaves beyond them; 0: tree
- * walk only).
- * Results do not depend on any of them. */
+ * walk only), and overlap (K = 2..16: the queries in K chunks, the walk of
+ * chunk c + 1 running while chunk c is expanded and scored, on two internal
+ * streams; 0: in sequence; FP64 and one-sided forms only).  Results do not
+ * depend on any of them. */
 #define MCLCCD_TUNE_EXPAND_GRID 0
 #define MCLCCD_TUNE_ACCD_GRID 1
 #define MCLCCD_TUNE_WALK_PACKET 2
 #define MCLCCD_TUNE_ACCD_REBIN 3
 #define MCLCCD_TUNE_WALK_WINDOW 4
-#define MCLCCD_TUNE_COUNT 5
+#define MCLCCD_TUNE_OVERLAP 5
+#define MCLCCD_TUNE_COUNT 6
 int mclccd_set_tuning(mclccd_tree *tree, int key, int value);
 int mclccd_get_tuning(const mclccd_tree *tree, int key, int *value);
 

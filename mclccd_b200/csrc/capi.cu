@@ -69,7 +69,12 @@ struct mclccd_tree {
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
     cudaEvent_t ev[8] = {};
-    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16};
+    // overlapped traverse (MCLCCD_TUNE_OVERLAP): walk and narrow-phase streams,
+    // fork / chunk / join events, per-chunk list boundaries
+    cudaStream_t s_walk = nullptr, s_narrow = nullptr;
+    cudaEvent_t ov_ev[4] = {};
+    DevBuf ovl;
+    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0};
 };
 
 namespace {
@@ -209,6 +214,59 @@ static int stage_ints(mclccd_tree *t, DevBuf &buf, DevBuf &tmp, const int *src, 
     return MCLCCD_OK;
 }
 
+// Overlapped traverse: the queries in `chunks` ranges.  The walk of chunk
+// c + 1 (high-priority stream) runs while chunk c's pairs are expanded and
+// scored (low-priority stream), so the latency-bound walk and the FP64-bound
+// narrow phase share the SMs.  Running counters are snapshotted between
+// launches (ovl: pair, VF and EE list ends per chunk) to give each launch its
+// range; the lists, hits and counts are the ones of the sequential order
+// (only their order in the buffers differs).
+template <typename Accd>
+static int enqueue_overlapped(mclccd_tree *t, int chunks, int dim, int np, int nv, const int *dP, const double *dV1,
+                              bool discr, Counters *cnt, Accd &accd)
+{
+    cudaStream_t st = t->stream;
+    if (!t->s_walk) {
+        int least = 0, greatest = 0;
+        MC_CUDA(t, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        MC_CUDA(t, cudaStreamCreateWithPriority(&t->s_walk, cudaStreamNonBlocking, greatest));
+        MC_CUDA(t, cudaStreamCreateWithPriority(&t->s_narrow, cudaStreamNonBlocking, least));
+        for (auto &e : t->ov_ev) MC_CUDA(t, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    MC_CUDA(t, ensure(t->ovl, sizeof(unsigned long long) * 3 * 17));
+    unsigned long long *pe = as<unsigned long long>(t->ovl), *ve = pe + 17, *ee = ve + 17;
+    MC_CUDA(t, cudaMemsetAsync(pe, 0, sizeof(unsigned long long) * 3 * 17, st));
+    MC_CUDA(t, cudaEventRecord(t->ov_ev[0], st));   // fork
+    MC_CUDA(t, cudaStreamWaitEvent(t->s_walk, t->ov_ev[0], 0));
+    MC_CUDA(t, cudaStreamWaitEvent(t->s_narrow, t->ov_ev[0], 0));
+    const int nq = np - 1;
+    for (int c = 0; c < chunks; ++c) {
+        const int qb = (int)((long long)nq * c / chunks), qe = (int)((long long)nq * (c + 1) / chunks);
+        launch_traverse(dim, 0, t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes), t->leaf_box.p,
+                        as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
+                        cnt, t->s_walk, qb, qe);
+        launch_snapshot(&cnt->n_pairs, pe + c + 1, nullptr, nullptr, t->s_walk);
+        MC_CUDA(t, cudaEventRecord(t->ov_ev[1], t->s_walk));
+        MC_CUDA(t, cudaStreamWaitEvent(t->s_narrow, t->ov_ev[1], 0));
+        launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                            as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc, 1,
+                            discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], t->s_narrow, pe + c, pe + c + 1);
+        launch_snapshot(&cnt->n_vf, ve + c + 1, &cnt->n_ee, ee + c + 1, t->s_narrow);
+        accd(true, t->vf, ve + c + 1, t->cap_vf, t->vf_eta, ve + c, t->s_narrow);
+        if (dim == 3) accd(false, t->ee, ee + c + 1, t->cap_ee, t->ee_eta, ee + c, t->s_narrow);
+        t->launches += 4;
+    }
+    MC_CUDA(t, cudaEventRecord(t->ov_ev[2], t->s_walk));   // join
+    MC_CUDA(t, cudaEventRecord(t->ov_ev[3], t->s_narrow));
+    MC_CUDA(t, cudaStreamWaitEvent(st, t->ov_ev[2], 0));
+    MC_CUDA(t, cudaStreamWaitEvent(st, t->ov_ev[3], 0));
+    if (t->flags & MCLCCD_OPT_PROFILE) {   // walk = all chunks' walks; expand = 0; narrow = the rest
+        cudaEventRecord(t->ev[4], t->s_walk);
+        cudaEventRecord(t->ev[5], t->s_walk);
+    }
+    return MCLCCD_OK;
+}
+
 extern "C" {
 
 const char *mclccd_status_string(int s)
@@ -260,6 +318,11 @@ int mclccd_destroy(mclccd_tree *t)
         if (b->p) cudaFree(b->p);
     for (int i = 0; i < 8; ++i)
         if (t->ev[i]) cudaEventDestroy(t->ev[i]);
+    for (int i = 0; i < 4; ++i)
+        if (t->ov_ev[i]) cudaEventDestroy(t->ov_ev[i]);
+    if (t->s_walk) cudaStreamDestroy(t->s_walk);
+    if (t->s_narrow) cudaStreamDestroy(t->s_narrow);
+    if (t->ovl.p) cudaFree(t->ovl.p);
     if (t->h_cnt) cudaFreeHost(t->h_cnt);
     if (t->h_diff) cudaFreeHost(t->h_diff);
     if (t->own_stream) cudaStreamDestroy(t->own_stream);
@@ -590,39 +653,44 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
         const bool certified = t->precision == MCLCCD_PREC_FP32_CERTIFIED;
         if (certified && cont) MC_CUDA(t, ensure(t->fp64_queue, sizeof(unsigned) * std::max(t->cap_vf, t->cap_ee)));
         MC_CUDA(t, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
-        launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes),
-                        t->leaf_box.p,
-                        as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
-                        cnt, st);
-        if (prof) cudaEventRecord(t->ev[4], st);
-        launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
-                            as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
-                            cont, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st);
-        if (prof) cudaEventRecord(t->ev[5], st);
-        t->launches += 2;
-        if (cont) {
-            // FP32-certified: an FP32 pass and an FP64 pass over its queue per list.
-            const bool one_sided = (t->flags & MCLCCD_OPT_VF_ONE_SIDED) != 0;
-            auto accd = [&](bool vf, DevBuf &list, unsigned long long *n_ptr, unsigned long long cap, double eta) {
-                if (vf && one_sided) {   // BVHTree.cpp:445-447: CTCD with the wrong-side test
-                    launch_ctcd_pipeline(dim, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
-                                         as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
-                                         t->tune[MCLCCD_TUNE_ACCD_GRID], st);
-                    ++t->launches;
-                } else if (certified) {
-                    launch_accd_certified(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
-                                          as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits,
-                                          as<unsigned>(t->fp64_queue), cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], st);
-                    t->launches += 2;
-                } else {
-                    launch_accd_pipeline(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
-                                         as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
-                                         t->tune[MCLCCD_TUNE_ACCD_GRID], t->tune[MCLCCD_TUNE_ACCD_REBIN] != 0, st);
-                    ++t->launches;
-                }
-            };
-            accd(true, t->vf, &cnt->n_vf, t->cap_vf, t->vf_eta);
-            if (dim == 3) accd(false, t->ee, &cnt->n_ee, t->cap_ee, t->ee_eta);
+        const bool one_sided = (t->flags & MCLCCD_OPT_VF_ONE_SIDED) != 0;
+        // narrow phase of one list, stencils [*lo, *n) (lo == nullptr: from 0)
+        auto accd = [&](bool vf, DevBuf &list, const unsigned long long *n_ptr, unsigned long long cap, double eta,
+                        const unsigned long long *lo, cudaStream_t s) {
+            if (vf && one_sided) {   // BVHTree.cpp:445-447: CTCD with the wrong-side test
+                launch_ctcd_pipeline(dim, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
+                                     as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
+                                     t->tune[MCLCCD_TUNE_ACCD_GRID], s, lo);
+                ++t->launches;
+            } else if (certified) {   // an FP32 pass and an FP64 pass over its queue
+                launch_accd_certified(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
+                                      as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits,
+                                      as<unsigned>(t->fp64_queue), cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], s);
+                t->launches += 2;
+            } else {
+                launch_accd_pipeline(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
+                                     as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
+                                     t->tune[MCLCCD_TUNE_ACCD_GRID], t->tune[MCLCCD_TUNE_ACCD_REBIN] != 0, s, lo);
+                ++t->launches;
+            }
+        };
+        const int chunks = t->tune[MCLCCD_TUNE_OVERLAP];
+        if (chunks >= 2 && cont && !certified && !t->tune[MCLCCD_TUNE_WALK_PACKET] && np > 2 * chunks * 128) {
+            if (int rc = enqueue_overlapped(t, chunks, dim, np, nv, dP, dV1, discr, cnt, accd)) return rc;
+        } else {
+            launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], t->tune[MCLCCD_TUNE_WALK_WINDOW],
+                            as<Node>(t->nodes), t->leaf_box.p, as<unsigned char>(t->leaf_active), as<int>(t->vals), np,
+                            as<int2>(t->pairs), t->cap_pairs, cnt, st);
+            if (prof) cudaEventRecord(t->ev[4], st);
+            launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                                as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc),
+                                t->cap_disc, cont, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st);
+            if (prof) cudaEventRecord(t->ev[5], st);
+            t->launches += 2;
+            if (cont) {
+                accd(true, t->vf, &cnt->n_vf, t->cap_vf, t->vf_eta, nullptr, st);
+                if (dim == 3) accd(false, t->ee, &cnt->n_ee, t->cap_ee, t->ee_eta, nullptr, st);
+            }
         }
         if (prof) cudaEventRecord(t->ev[6], st);
         if (int rc = check_launch(t, "traverse kernels")) return rc;
@@ -998,7 +1066,9 @@ int mclccd_set_tuning(mclccd_tree *t, int key, int value)
 {
     if (!t || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
     const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_ACCD_REBIN;
-    if (key == MCLCCD_TUNE_WALK_WINDOW) {
+    if (key == MCLCCD_TUNE_OVERLAP) {
+        if (value < 0 || value > 16) return fail(t, MCLCCD_ERR_INVALID, "overlap chunks must be in [0, 16]");
+    } else if (key == MCLCCD_TUNE_WALK_WINDOW) {
         if (value != 0 && value != 8 && value != 16 && value != 32 && value != 64 && value != 128)
             return fail(t, MCLCCD_ERR_INVALID, "walk window must be 0, 8, 16, 32, 64 or 128");
     } else if (flag ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))

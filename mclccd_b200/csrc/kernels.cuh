@@ -25,18 +25,23 @@ void launch_sort_pairs(unsigned *keys, int *vals, unsigned *keys_alt, int *vals_
                        void *scratch, Counters *cnt, cudaStream_t st);
 
 // traverse.cu
+// queries [q_begin, q_end) (q_end < 0: to the end)
 void launch_traverse(int dim, int packet, int window, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
-                     const int *sorted, int n, int2 *pairs, unsigned long long cap, Counters *cnt, cudaStream_t st);
+                     const int *sorted, int n, int2 *pairs, unsigned long long cap, Counters *cnt, cudaStream_t st,
+                     int q_begin = 0, int q_end = -1);
 void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,
                          const unsigned char *flags, const double *V1, int nv, int4 *vf, unsigned long long vf_cap,
                          int4 *ee, unsigned long long ee_cap, int2 *disc, unsigned long long disc_cap, int continuous,
-                         int discrete, Counters *cnt, int grid, cudaStream_t st);
+                         int discrete, Counters *cnt, int grid, cudaStream_t st,
+                         const unsigned long long *lo_ptr = nullptr, const unsigned long long *hi_ptr = nullptr);
+void launch_snapshot(const unsigned long long *a, unsigned long long *da, const unsigned long long *b,
+                     unsigned long long *db, cudaStream_t st);
 
 // narrow.cu
 void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
                           unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, bool rebin,
-                          cudaStream_t st);
+                          cudaStream_t st, const unsigned long long *lo_ptr = nullptr);
 // certified.cu
 void launch_accd_certified(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr,
                            unsigned long long cap, const double *V0, const double *V1, int nv, double eta,
@@ -56,6 +61,7 @@ void launch_accd_bulk(int dim, const int *sten, const unsigned char *is_vf, long
 // narrow.cu: one-sided VF narrow phase (CTCD) over the VF list
 void launch_ctcd_pipeline(int dim, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
-                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st);
+                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st,
+                          const unsigned long long *lo_ptr = nullptr);
 
 } // namespace mclccd

@@ -43,12 +43,14 @@ __global__ void __launch_bounds__(128, MCLCCD_ACCD_MIN_BLOCKS)
 k_accd_pipeline(const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
                 const double *__restrict__ V0, const double *__restrict__ V1, int nv, double eta,
                 int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,
-                unsigned long long hit_cap, Counters *cnt)
+                unsigned long long hit_cap, Counters *cnt, const unsigned long long *lo_ptr)
 {
+    // stencils [lo, n): the whole list, or one query chunk's part of it
     unsigned long long n = *(volatile const unsigned long long *)n_ptr;
     if (n > cap) n = cap;
+    const unsigned long long lo = lo_ptr ? min(*(volatile const unsigned long long *)lo_ptr, n) : 0ull;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (unsigned long long i = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const int4 s4 = sten[i];
         const int s[4] = {s4.x, s4.y, s4.z, s4.w};
         double x0[DIM + 1][DIM], x1[DIM + 1][DIM];
@@ -102,7 +104,7 @@ __global__ void __launch_bounds__(kRebinBlock, MCLCCD_ACCD_MIN_BLOCKS)
 k_accd_rebin(const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
              const double *__restrict__ V0, const double *__restrict__ V1, int nv, double eta,
              int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,
-             unsigned long long hit_cap, Counters *cnt)
+             unsigned long long hit_cap, Counters *cnt, const unsigned long long *lo_ptr)
 {
     __shared__ int4 q_sten[2 * kRebinBlock];
     __shared__ double q_d0[2 * kRebinBlock], q_lp[2 * kRebinBlock];
@@ -129,8 +131,9 @@ k_accd_rebin(const int4 *__restrict__ sten, const unsigned long long *n_ptr, uns
         if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
         return hit && toi >= 0.0 ? toi : -1.0;
     };
+    const unsigned long long lo = lo_ptr ? min(*(volatile const unsigned long long *)lo_ptr, n) : 0ull;
     const unsigned long long stride = (unsigned long long)gridDim.x * kRebinBlock;
-    for (unsigned long long base = (unsigned long long)blockIdx.x * kRebinBlock; base < n; base += stride) {
+    for (unsigned long long base = lo + (unsigned long long)blockIdx.x * kRebinBlock; base < n; base += stride) {
         const unsigned long long i = base + tid;
         int4 s4 = make_int4(0, 0, 0, 0);
         double toi = -1.0;
@@ -203,12 +206,13 @@ __global__ void __launch_bounds__(128)
 k_ctcd_pipeline(const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
                 const double *__restrict__ V0, const double *__restrict__ V1, int nv, double eta,
                 int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,
-                unsigned long long hit_cap, Counters *cnt)
+                unsigned long long hit_cap, Counters *cnt, const unsigned long long *lo_ptr)
 {
     unsigned long long n = *(volatile const unsigned long long *)n_ptr;
     if (n > cap) n = cap;
+    const unsigned long long lo = lo_ptr ? min(*(volatile const unsigned long long *)lo_ptr, n) : 0ull;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (unsigned long long i = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const int4 s4 = sten[i];
         const int s[4] = {s4.x, s4.y, s4.z, s4.w};
         double x0[DIM + 1][DIM], x1[DIM + 1][DIM];
@@ -259,22 +263,22 @@ k_accd_bulk(const int *__restrict__ sten, const unsigned char *__restrict__ is_v
 void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
                           unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, bool rebin,
-                          cudaStream_t st)
+                          cudaStream_t st, const unsigned long long *lo_ptr)
 {
     if (rebin) {
         if (dim == 3) {
-            if (vf) k_accd_rebin<3, true><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
-            else k_accd_rebin<3, false><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+            if (vf) k_accd_rebin<3, true><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt, lo_ptr);
+            else k_accd_rebin<3, false><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt, lo_ptr);
         } else {
-            k_accd_rebin<2, true><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+            k_accd_rebin<2, true><<<grid, kRebinBlock, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt, lo_ptr);
         }
         return;
     }
     if (dim == 3) {
-        if (vf) k_accd_pipeline<3, true><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
-        else k_accd_pipeline<3, false><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+        if (vf) k_accd_pipeline<3, true><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt, lo_ptr);
+        else k_accd_pipeline<3, false><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt, lo_ptr);
     } else {
-        k_accd_pipeline<2, true><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+        k_accd_pipeline<2, true><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt, lo_ptr);
     }
 }
 
@@ -296,10 +300,11 @@ void launch_accd_bulk(int dim, const int *sten, const unsigned char *is_vf, long
 
 void launch_ctcd_pipeline(int dim, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
-                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st)
+                          unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, cudaStream_t st,
+                          const unsigned long long *lo_ptr)
 {
-    if (dim == 3) k_ctcd_pipeline<3><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
-    else k_ctcd_pipeline<2><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt);
+    if (dim == 3) k_ctcd_pipeline<3><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt, lo_ptr);
+    else k_ctcd_pipeline<2><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt, lo_ptr);
 }
 
 } // namespace mclccd

@@ -31,12 +31,12 @@ constexpr int kStackDepth = MCLCCD_WALK_STACK;
 template <int DIM>
 __global__ void __launch_bounds__(128, MCLCCD_WALK_MIN_BLOCKS)
 k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
-           const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
-           int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
+           const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n, int q_begin,
+           int q_end, int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
 {
     constexpr int S = DIM == 3 ? 3 : 2;
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n - 1) return;
+    const int q = q_begin + blockIdx.x * blockDim.x + threadIdx.x;   // queries [q_begin, q_end), q_end <= n - 1
+    if (q >= q_end) return;
     const bool qact = leaf_active[q] != 0;
     const int qprim = sorted[q];
     // Only the FP32 boxes stay in registers; the FP64 box is re-read for the
@@ -124,8 +124,8 @@ k_traverse(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf
 template <int DIM, int W>
 __global__ void __launch_bounds__(128, 4)
 k_traverse_window(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
-                  const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
-                  int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
+                  const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n, int q_begin,
+                  int q_end, int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
 {
     constexpr int S = DIM == 3 ? 3 : 2;
     constexpr int NB = 127 + W;
@@ -133,8 +133,8 @@ k_traverse_window(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict
     __shared__ unsigned char s_act[NB];
     __shared__ int stack[kStackDepth][128];
     const int tid = threadIdx.x;
-    const int q0 = blockIdx.x * 128;
-    if (q0 >= n - 1) return;   // whole block past the end
+    const int q0 = q_begin + blockIdx.x * 128;   // queries [q_begin, q_end), q_end <= n - 1
+    if (q0 >= q_end) return;                      // whole block past the end
     for (int i = tid; i < NB; i += 128) {
         const int k = q0 + 1 + i;
         if (k < n) {
@@ -151,7 +151,7 @@ k_traverse_window(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict
     }
     __syncthreads();
     const int q = q0 + tid;
-    if (q >= n - 1) return;
+    if (q >= q_end) return;
     const bool qact = leaf_active[q] != 0;
     const int qprim = sorted[q];
     Box2T<DIM> qbox;
@@ -310,12 +310,16 @@ __global__ void __launch_bounds__(256)
 k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, const int *__restrict__ P,
                const unsigned char *__restrict__ flags, const double *__restrict__ V1, int nv,
                int4 *__restrict__ vf, unsigned long long vf_cap, int4 *__restrict__ ee, unsigned long long ee_cap,
-               int2 *__restrict__ disc, unsigned long long disc_cap, int continuous, int discrete, Counters *cnt)
+               int2 *__restrict__ disc, unsigned long long disc_cap, int continuous, int discrete, Counters *cnt,
+               const unsigned long long *lo_ptr, const unsigned long long *hi_ptr)
 {
-    unsigned long long n = *(volatile unsigned long long *)&cnt->n_pairs;
+    // pairs [lo, hi): the whole list, or one query chunk's part of it
+    unsigned long long n = *(volatile const unsigned long long *)hi_ptr;
     if (n > pair_cap) n = pair_cap;
+    unsigned long long lo = lo_ptr ? *(volatile const unsigned long long *)lo_ptr : 0ull;
+    if (lo > n) lo = n;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    for (unsigned long long base = lo + (unsigned long long)blockIdx.x * blockDim.x; base < n; base += stride) {
         const unsigned long long idx = base + threadIdx.x;
         const bool valid = idx < n;
         int2 pr = make_int2(0, 0);
@@ -379,10 +383,12 @@ k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, cons
 
 void launch_traverse(int dim, int packet, int window, const Node *nodes, const void *leaf_box,
                      const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs, unsigned long long cap,
-                     Counters *cnt, cudaStream_t st)
+                     Counters *cnt, cudaStream_t st, int q_begin, int q_end)
 {
     if (n < 2) return;
-    const int g = (n - 1 + 127) / 128;
+    if (q_end < 0 || q_end > n - 1) q_end = n - 1;
+    if (q_begin >= q_end) return;
+    const int g = (q_end - q_begin + 127) / 128;
     const auto *lb3 = reinterpret_cast<const LeafBox<3> *>(leaf_box);
     const auto *lb2 = reinterpret_cast<const LeafBox<2> *>(leaf_box);
     if (window) {
@@ -390,8 +396,12 @@ void launch_traverse(int dim, int packet, int window, const Node *nodes, const v
     case Wv:                                                                                                       \
         cudaFuncSetAttribute(k_traverse_window<3, Wv>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);        \
         cudaFuncSetAttribute(k_traverse_window<2, Wv>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);        \
-        if (dim == 3) k_traverse_window<3, Wv><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, pairs, cap, cnt); \
-        else k_traverse_window<2, Wv><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, pairs, cap, cnt);         \
+        if (dim == 3)                                                                                              \
+            k_traverse_window<3, Wv><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, q_begin, q_end, pairs,  \
+                                                         cap, cnt);                                                 \
+        else                                                                                                       \
+            k_traverse_window<2, Wv><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, q_begin, q_end, pairs,  \
+                                                         cap, cnt);                                                 \
         return;
         switch (window) {
             MCLCCD_WINDOW_CASE(8)
@@ -406,22 +416,38 @@ void launch_traverse(int dim, int packet, int window, const Node *nodes, const v
         if (dim == 3) k_traverse_packet<3><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, pairs, cap, cnt);
         else k_traverse_packet<2><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, pairs, cap, cnt);
     } else {
-        if (dim == 3) k_traverse<3><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, pairs, cap, cnt);
-        else k_traverse<2><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, pairs, cap, cnt);
+        if (dim == 3) k_traverse<3><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, q_begin, q_end, pairs, cap, cnt);
+        else k_traverse<2><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, q_begin, q_end, pairs, cap, cnt);
     }
 }
 
 void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,
                          const unsigned char *flags, const double *V1, int nv, int4 *vf, unsigned long long vf_cap,
                          int4 *ee, unsigned long long ee_cap, int2 *disc, unsigned long long disc_cap, int continuous,
-                         int discrete, Counters *cnt, int grid, cudaStream_t st)
+                         int discrete, Counters *cnt, int grid, cudaStream_t st, const unsigned long long *lo_ptr,
+                         const unsigned long long *hi_ptr)
 {
+    if (!hi_ptr) hi_ptr = &cnt->n_pairs;
     if (dim == 3)
         k_expand_pairs<3><<<grid, 256, 0, st>>>(pairs, pair_cap, P, flags, V1, nv, vf, vf_cap, ee, ee_cap, disc,
-                                                disc_cap, continuous, discrete, cnt);
+                                                disc_cap, continuous, discrete, cnt, lo_ptr, hi_ptr);
     else
         k_expand_pairs<2><<<grid, 256, 0, st>>>(pairs, pair_cap, P, flags, V1, nv, vf, vf_cap, ee, ee_cap, disc,
-                                                disc_cap, continuous, discrete, cnt);
+                                                disc_cap, continuous, discrete, cnt, lo_ptr, hi_ptr);
+}
+
+// dst[i] = *src[i]: a snapshot of running counters between two launches.
+__global__ void k_snapshot(const unsigned long long *a, unsigned long long *da, const unsigned long long *b,
+                           unsigned long long *db)
+{
+    *da = *(volatile const unsigned long long *)a;
+    if (b) *db = *(volatile const unsigned long long *)b;
+}
+
+void launch_snapshot(const unsigned long long *a, unsigned long long *da, const unsigned long long *b,
+                     unsigned long long *db, cudaStream_t st)
+{
+    k_snapshot<<<1, 1, 0, st>>>(a, da, b, db);
 }
 
 } // namespace mclccd

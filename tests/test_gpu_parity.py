@@ -87,6 +87,23 @@ def test_cfg0_folded_cloth(port):
     check_against_port(t, port, V0, V1, F, eta)
 
 
+@pytest.mark.parametrize("chunks", [2, 5])
+@pytest.mark.parametrize("scene", ["wavy", "annulus"])
+def test_overlapped_traverse_against_port(port, chunks, scene):
+    # walk of one query chunk overlapped with the narrow phase of the previous
+    # one: same candidates, hits (bit-identical toi) and discrete pairs
+    V0, V1, F, eta = scenes.wavy_cloth(1025, rows=97, seed=7) if scene == "wavy" else scenes.annulus_2d(800, seed=8)
+    t = BVHTree(V0.shape[1])
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.set_tuning(overlap=chunks)
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    check_against_port(t, port, V0, V1, F, eta)
+    t.update(V0, V1, F)
+    t.traverse()
+    check_against_port(t, port, V0, V1, F, eta)
+
+
 @pytest.mark.parametrize("window", [32, 128])
 @pytest.mark.parametrize("scene", ["wavy", "annulus", "active"])
 def test_walk_window_against_port(port, window, scene):
