@@ -1100,7 +1100,7 @@ void enqueue_build(mclccd_batch *b, GroupHost &G, cudaStream_t st)
 template <int DIM, bool CERT>
 void enqueue_accd(const BatchGroupDev &g, GroupHost &G, cudaStream_t st)
 {
-    const int grid = 148 * 16;
+    const int grid = 148 * 128;   // as the single-scene ACCD grid
     k_b_accd<DIM, true, CERT><<<grid, 128, 0, st>>>(g, G.w_vf, &G.w_cnt->n_vf, G.cap_vf, G.vert_scene);
     if constexpr (DIM == 3)
         k_b_accd<DIM, false, CERT><<<grid, 128, 0, st>>>(g, G.w_ee, &G.w_cnt->n_ee, G.cap_ee, G.vert_scene);
@@ -1124,7 +1124,7 @@ void enqueue_wave(mclccd_batch *b, GroupHost &G, cudaStream_t st)
     }
     k_wave_check_pairs<<<1, 1, 0, st>>>(G.ws, G.w_cnt, G.cap_pairs);
     launch_expand_pairs(G.dim, G.w_pairs, G.cap_pairs, G.P, G.flags, G.V1, G.nv, G.w_vf, G.cap_vf, G.w_ee, G.cap_ee,
-                        G.w_disc, G.cap_disc, 1, 1, G.w_cnt, 148 * 8, st);
+                        G.w_disc, G.cap_disc, 1, 1, G.w_cnt, 148 * 16, st);
     k_wave_check_sten<<<1, 1, 0, st>>>(G.ws, G.w_cnt, G.cap_vf, G.cap_ee, G.cap_disc);
     const bool cert = b->precision == MCLCCD_PREC_FP32_CERTIFIED;
     if (G.dim == 3) { if (cert) enqueue_accd<3, true>(g, G, st); else enqueue_accd<3, false>(g, G, st); }
