@@ -99,6 +99,20 @@ int mclccd_update(mclccd_tree *tree, const double *V0, const double *V1, int nv,
  * Results stay on the device until read with mclccd_get_*. */
 int mclccd_traverse(mclccd_tree *tree, const double *V0, const double *V1, int nv, const int *P, int mem_kind);
 
+/* traverse and deliver the results into caller buffers in one call, as the
+ * reference's traverse hands each hit to append_pair and each discrete pair
+ * to append_discrete (BVHTree.cpp:262-281): hits (stencil int32 x 4, is_vf,
+ * toi) and discrete pairs (int32 x 2) are written to the out_* arrays on the
+ * out_mem_kind side, at most the given capacities (a prefix), in the order
+ * of mclccd_get_hits / mclccd_get_discrete; n_hits / n_discrete receive the
+ * full counts.  Host outputs are copied in chunks while later chunks of the
+ * step compute (page-locked buffers let the copies overlap).  Any out_*
+ * pointer may be NULL. */
+int mclccd_traverse_out(mclccd_tree *tree, const double *V0, const double *V1, int nv, const int *P, int mem_kind,
+                        int *out_sten, unsigned char *out_is_vf, double *out_toi, long long hit_capacity,
+                        long long *n_hits, int *out_discrete, long long disc_capacity, long long *n_discrete,
+                        int out_mem_kind);
+
 /* Counts from the last traverse: CCD hits (append_pair calls), discrete
  * pairs (append_discrete calls), candidate VF / EE stencils (filter_pair
  * calls) and leaf pairs whose boxes intersect.  Any pointer may be NULL. */

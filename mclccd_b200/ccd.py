@@ -66,6 +66,8 @@ def lib():
         "mclccd_update_f32": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int], C.c_int),
         "mclccd_update_ex": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int, C.c_uint], C.c_int),
         "mclccd_traverse_ex": ([vp, vp, vp, C.c_int, vp, C.c_int, C.c_uint], C.c_int),
+        "mclccd_traverse_out": ([vp, vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, C.c_longlong, llp, vp, C.c_longlong, llp,
+                                 C.c_int], C.c_int),
         "mclccd_traverse_f32": ([vp, vp, vp, C.c_int, vp, C.c_int], C.c_int),
         "mclccd_counts": ([vp, llp, llp, llp, llp, llp], C.c_int),
         "mclccd_get_hits": ([vp, C.c_int, C.c_longlong, vp, vp, vp], C.c_int),
@@ -290,6 +292,40 @@ class BVHTree:
         if V0 is not None:
             self._nv = nv
         self._dispatch(V0, V1)
+
+    def traverse_out(self, sten, is_vf, toi, discrete=None, V0=None, V1=None, P=None):
+        """traverse with the results delivered into caller arrays
+        (mclccd_traverse_out): sten (cap x 4 int32), is_vf (cap uint8), toi
+        (cap float64), discrete (dcap x 2 int32), all host (numpy / CPU
+        tensors, page-locked for overlap) or all CUDA tensors.  Host copies
+        overlap the rest of the step.  Returns (n_hits, n_discrete), the
+        full counts; the arrays receive a prefix up to their capacity.  The
+        hooks are not called."""
+        pv0, k0, a0, nv = _arg(V0, np.float64, self.dim)
+        pv1, k1, a1, _ = _arg(V1, np.float64, self.dim)
+        pp, kp, ap, _ = _arg(P, np.int32)
+        kind = k0 if k0 is not None else MEM_HOST
+
+        def ptr(a):
+            if a is None:
+                return None, None
+            if hasattr(a, "data_ptr"):
+                return C.c_void_p(a.data_ptr()), (MEM_DEVICE if a.is_cuda else MEM_HOST)
+            return C.c_void_p(a.ctypes.data), MEM_HOST
+        (ps, ks), (pv, kv), (pt, kt) = ptr(sten), ptr(is_vf), ptr(toi)
+        pd, kd = ptr(discrete)
+        kinds = {k for k in (ks, kv, kt, kd) if k is not None}
+        if len(kinds) > 1:
+            raise ValueError("output arrays must all be host arrays or all CUDA tensors")
+        cap = min(len(x) for x in (sten, is_vf, toi) if x is not None) if any(x is not None for x in (sten, is_vf, toi)) else 0
+        dcap = len(discrete) if discrete is not None else 0
+        nh, nd = C.c_longlong(), C.c_longlong()
+        self._push_options()
+        self._check(self._L.mclccd_traverse_out(self._h, pv0, pv1, nv, pp, kind, ps, pv, pt, cap, C.byref(nh), pd, dcap,
+                                                C.byref(nd), kinds.pop() if kinds else MEM_HOST), self._h)
+        if V0 is not None:
+            self._nv = nv
+        return nh.value, nd.value
 
     def _dispatch(self, V0, V1):
         if self.filter_pair is not None or self.narrow_phase is not None:

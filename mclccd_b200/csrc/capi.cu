@@ -78,6 +78,12 @@ struct mclccd_tree {
     cudaStream_t s_walk = nullptr, s_narrow = nullptr;
     cudaEvent_t ov_ev[4] = {};
     DevBuf ovl;
+    // streamed results (mclccd_traverse_out): copy stream, per-chunk events
+    // and pinned hit-count snapshots
+    cudaStream_t s_copy = nullptr;
+    cudaEvent_t out_ev[16] = {};
+    unsigned long long *h_snap = nullptr;
+    unsigned long long out_done = 0;   // hits already copied out by the streamed path
     int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0};
 };
 
@@ -271,6 +277,108 @@ static int enqueue_overlapped(mclccd_tree *t, int chunks, int dim, int np, int n
     return MCLCCD_OK;
 }
 
+// Caller buffers for the results of mclccd_traverse_out.
+struct HostOut {
+    int *sten;
+    unsigned char *is_vf;
+    double *toi;
+    long long hit_cap;
+    int *disc;
+    long long disc_cap;
+    int mem_kind;
+};
+
+// mclccd_traverse_out: the step in kOutChunks query chunks on the handle's
+// stream; after each chunk's narrow phase its hits (appended after the
+// previous chunks') are copied to the caller's host arrays on a copy stream
+// while the next chunks compute.  The host waits on each chunk's event to
+// learn its hit count (a pinned snapshot).  Copies stop at the caller's
+// capacity; an overflow retry recomputes and copies again from the start.
+constexpr int kOutChunks = 8;
+
+template <typename Accd>
+static int enqueue_streamed(mclccd_tree *t, int dim, int np, int nv, const int *dP, const double *dV1, bool discr,
+                            Counters *cnt, Accd &accd, const HostOut &out)
+{
+    cudaStream_t st = t->stream;
+    if (!t->s_copy) {
+        MC_CUDA(t, cudaStreamCreateWithFlags(&t->s_copy, cudaStreamNonBlocking));
+        for (auto &e : t->out_ev) MC_CUDA(t, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        MC_CUDA(t, cudaHostAlloc(reinterpret_cast<void **>(&t->h_snap), sizeof(unsigned long long) * 16, 0));
+    }
+    MC_CUDA(t, ensure(t->ovl, sizeof(unsigned long long) * 3 * 17));
+    unsigned long long *pe = as<unsigned long long>(t->ovl), *ve = pe + 17, *ee = ve + 17;
+    MC_CUDA(t, cudaMemsetAsync(pe, 0, sizeof(unsigned long long) * 3 * 17, st));
+    const int nq = np - 1;
+    for (int c = 0; c < kOutChunks; ++c) {
+        const int qb = (int)((long long)nq * c / kOutChunks), qe = (int)((long long)nq * (c + 1) / kOutChunks);
+        launch_traverse(dim, 0, t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes), t->leaf_box.p,
+                        as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
+                        cnt, st, qb, qe);
+        launch_snapshot(&cnt->n_pairs, pe + c + 1, nullptr, nullptr, st);
+        launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                            as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc, 1,
+                            discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st, pe + c, pe + c + 1);
+        launch_snapshot(&cnt->n_vf, ve + c + 1, &cnt->n_ee, ee + c + 1, st);
+        accd(true, t->vf, ve + c + 1, t->cap_vf, t->vf_eta, ve + c, st);
+        if (dim == 3) accd(false, t->ee, ee + c + 1, t->cap_ee, t->ee_eta, ee + c, st);
+        t->launches += 4;
+        MC_CUDA(t, cudaMemcpyAsync(t->h_snap + c, &cnt->n_hits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        MC_CUDA(t, cudaEventRecord(t->out_ev[c], st));
+    }
+    if (t->flags & MCLCCD_OPT_PROFILE) {   // walk = the whole chunked step; expand, narrow = 0
+        cudaEventRecord(t->ev[4], st);
+        cudaEventRecord(t->ev[5], st);
+    }
+    if (int rc = check_launch(t, "traverse kernels")) return rc;
+    // stream each chunk's hits out as soon as it is done
+    unsigned long long done = 0;
+    const unsigned long long lim = std::min<unsigned long long>((unsigned long long)std::max(out.hit_cap, 0ll),
+                                                                t->cap_hits);
+    for (int c = 0; c < kOutChunks; ++c) {
+        MC_CUDA(t, cudaEventSynchronize(t->out_ev[c]));
+        const unsigned long long upto = std::min<unsigned long long>(t->h_snap[c], lim);
+        if (upto <= done) continue;
+        const size_t n = (size_t)(upto - done);
+        if (out.sten)
+            MC_CUDA(t, cudaMemcpyAsync(out.sten + 4 * done, as<int4>(t->hit_sten) + done, sizeof(int4) * n,
+                                       cudaMemcpyDeviceToHost, t->s_copy));
+        if (out.is_vf)
+            MC_CUDA(t, cudaMemcpyAsync(out.is_vf + done, as<unsigned char>(t->hit_isvf) + done, n,
+                                       cudaMemcpyDeviceToHost, t->s_copy));
+        if (out.toi)
+            MC_CUDA(t, cudaMemcpyAsync(out.toi + done, as<double>(t->hit_toi) + done, sizeof(double) * n,
+                                       cudaMemcpyDeviceToHost, t->s_copy));
+        done = upto;
+    }
+    t->out_done = done;
+    return MCLCCD_OK;
+}
+
+// The results of a successful traverse_out into the caller's buffers: the
+// hits not streamed yet, then the discrete pairs.
+static int deliver_out(mclccd_tree *t, const HostOut &out)
+{
+    cudaStream_t st = t->stream;
+    const unsigned long long nh = std::min<unsigned long long>(t->n_hits, (unsigned long long)std::max(out.hit_cap, 0ll));
+    const cudaMemcpyKind k = out.mem_kind == MCLCCD_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    const unsigned long long from = t->out_done < nh ? t->out_done : nh;
+    if (nh > from) {
+        const size_t n = (size_t)(nh - from);
+        if (out.sten)
+            MC_CUDA(t, cudaMemcpyAsync(out.sten + 4 * from, as<int4>(t->hit_sten) + from, sizeof(int4) * n, k, st));
+        if (out.is_vf) MC_CUDA(t, cudaMemcpyAsync(out.is_vf + from, as<unsigned char>(t->hit_isvf) + from, n, k, st));
+        if (out.toi)
+            MC_CUDA(t, cudaMemcpyAsync(out.toi + from, as<double>(t->hit_toi) + from, sizeof(double) * n, k, st));
+    }
+    const unsigned long long nd = std::min<unsigned long long>(t->n_disc, (unsigned long long)std::max(out.disc_cap, 0ll));
+    if (out.disc && nd) MC_CUDA(t, cudaMemcpyAsync(out.disc, t->disc.p, sizeof(int2) * nd, k, st));
+    if (t->s_copy) MC_CUDA(t, cudaStreamSynchronize(t->s_copy));
+    MC_CUDA(t, cudaStreamSynchronize(st));
+    t->out_done = 0;
+    return MCLCCD_OK;
+}
+
 extern "C" {
 
 const char *mclccd_status_string(int s)
@@ -325,6 +433,10 @@ int mclccd_destroy(mclccd_tree *t)
     for (int i = 0; i < 4; ++i)
         if (t->ov_ev[i]) cudaEventDestroy(t->ov_ev[i]);
     if (t->s_walk) cudaStreamDestroy(t->s_walk);
+    if (t->s_copy) cudaStreamSynchronize(t->s_copy), cudaStreamDestroy(t->s_copy);
+    for (auto e : t->out_ev)
+        if (e) cudaEventDestroy(e);
+    if (t->h_snap) cudaFreeHost(t->h_snap);
     if (t->s_narrow) cudaStreamDestroy(t->s_narrow);
     if (t->ovl.p) cudaFree(t->ovl.p);
     if (t->h_cnt) cudaFreeHost(t->h_cnt);
@@ -586,9 +698,18 @@ int mclccd_traverse_f32(mclccd_tree *t, const float *V0, const float *V1, int nv
     return mclccd_traverse_ex(t, V0, V1, nv, P, mem_kind, MCLCCD_IN_F32);
 }
 
+static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int nv, const int *P, int mem_kind,
+                         const HostOut *out);
+
 int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, const int *P, int mem_kind)
 {
     if (!t) return MCLCCD_ERR_INVALID;
+    return traverse_impl(t, V0, V1, nv, P, mem_kind, nullptr);
+}
+
+static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int nv, const int *P, int mem_kind,
+                         const HostOut *out)
+{
     t->err.clear();
     if (!t->built) return fail(t, MCLCCD_ERR_STATE, "traverse before a successful update");
     if (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE) return fail(t, MCLCCD_ERR_INVALID, "bad mem_kind");
@@ -679,7 +800,12 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
             }
         };
         const int chunks = t->tune[MCLCCD_TUNE_OVERLAP];
-        if (chunks >= 2 && cont && !certified && !t->tune[MCLCCD_TUNE_WALK_PACKET] && np > 2 * chunks * 128) {
+        // host results stream out chunk by chunk while later chunks compute
+        const bool stream_out = out && out->mem_kind == MCLCCD_MEM_HOST && cont && !certified &&
+                                !t->tune[MCLCCD_TUNE_WALK_PACKET] && np > 2 * kOutChunks * 128;
+        if (stream_out) {
+            if (int rc = enqueue_streamed(t, dim, np, nv, dP, dV1, discr, cnt, accd, *out)) return rc;
+        } else if (chunks >= 2 && cont && !certified && !t->tune[MCLCCD_TUNE_WALK_PACKET] && np > 2 * chunks * 128) {
             if (int rc = enqueue_overlapped(t, chunks, dim, np, nv, dP, dV1, discr, cnt, accd)) return rc;
         } else {
             launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], t->tune[MCLCCD_TUNE_WALK_WINDOW],
@@ -735,10 +861,31 @@ int mclccd_traverse(mclccd_tree *t, const double *V0, const double *V1, int nv, 
     // iterations (the reference then reports a hit too); it is not a failure.
     const unsigned fatal = c.err & ~kErrAccdIters;
     if (fatal) {
+        if (t->s_copy) cudaStreamSynchronize(t->s_copy);
         t->traversed = false;
         return device_errors(t, fatal);
     }
+    if (out) {
+        if (int rc = deliver_out(t, *out)) return rc;
+    }
     return MCLCCD_OK;
+}
+
+int mclccd_traverse_out(mclccd_tree *t, const double *V0, const double *V1, int nv, const int *P, int mem_kind,
+                        int *out_sten, unsigned char *out_is_vf, double *out_toi, long long hit_capacity,
+                        long long *n_hits, int *out_discrete, long long disc_capacity, long long *n_discrete,
+                        int out_mem_kind)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (out_mem_kind != MCLCCD_MEM_HOST && out_mem_kind != MCLCCD_MEM_DEVICE)
+        return fail(t, MCLCCD_ERR_INVALID, "bad output mem_kind");
+    if (hit_capacity < 0 || disc_capacity < 0) return fail(t, MCLCCD_ERR_INVALID, "negative capacity");
+    HostOut out{out_sten, out_is_vf, out_toi, hit_capacity, out_discrete, disc_capacity, out_mem_kind};
+    t->out_done = 0;
+    const int rc = traverse_impl(t, V0, V1, nv, P, mem_kind, &out);
+    if (n_hits) *n_hits = rc == MCLCCD_OK ? (long long)t->n_hits : 0;
+    if (n_discrete) *n_discrete = rc == MCLCCD_OK ? (long long)t->n_disc : 0;
+    return rc;
 }
 
 int mclccd_counts(const mclccd_tree *t, long long *n_hits, long long *n_discrete, long long *n_vf, long long *n_ee,

@@ -87,6 +87,41 @@ def test_cfg0_folded_cloth(port):
     check_against_port(t, port, V0, V1, F, eta)
 
 
+def test_traverse_out_delivers_the_results(port):
+    # mclccd_traverse_out: results streamed into caller arrays (host copies
+    # overlapping the chunked step) equal the traverse + get_hits results
+    torch = pytest.importorskip("torch")
+    V0, V1, F, eta = scenes.wavy_cloth(1025, rows=161, seed=9)
+    t = BVHTree(3)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    p = check_against_port(t, port, V0, V1, F, eta)
+    want = hit_map(*t.hits())
+    wd = sort_rows(t.discrete())
+    n = len(want)
+    cap = n + 100
+    hs = torch.empty((cap, 4), dtype=torch.int32).pin_memory()
+    hv = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    ht = torch.empty(cap, dtype=torch.float64).pin_memory()
+    hd = torch.empty((len(wd) + 10, 2), dtype=torch.int32).pin_memory()
+    nh, nd = t.traverse_out(hs, hv, ht, hd, V0, V1, F)
+    assert (nh, nd) == (n, len(wd))
+    assert hit_map(hs[:nh].numpy(), hv[:nh].numpy(), ht[:nh].numpy()) == want
+    assert np.array_equal(sort_rows(hd[:nd].numpy()), wd)
+    # refit-only step, outputs on the device
+    t.update(V0, V1, F)
+    ds, dv, dt = (torch.empty_like(x, device="cuda") for x in (hs, hv, ht))
+    nh2, _ = t.traverse_out(ds, dv, dt)
+    assert nh2 == n and hit_map(ds[:n].cpu().numpy(), dv[:n].cpu().numpy(), dt[:n].cpu().numpy()) == want
+    # a capacity below the count: a prefix, the full count reported
+    small = n // 3
+    nh3, _ = t.traverse_out(hs[:small], hv[:small], ht[:small])
+    assert nh3 == n
+    got = hit_map(hs[:small].numpy(), hv[:small].numpy(), ht[:small].numpy())
+    assert len(got) == small and all(want[k] == v for k, v in got.items())
+
+
 @pytest.mark.parametrize("chunks", [2, 5])
 @pytest.mark.parametrize("scene", ["wavy", "annulus"])
 def test_overlapped_traverse_against_port(port, chunks, scene):
