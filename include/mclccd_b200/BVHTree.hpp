@@ -24,6 +24,7 @@
 #include <array>
 #include <cmath>
 #include <limits>
+#include <memory>
 #include <type_traits>
 #include <functional>
 #include <stdexcept>
@@ -112,6 +113,9 @@ public:
     {
         auto *self = const_cast<BVHTree *>(this);
         self->push_options();
+        if constexpr (!kFloat) {
+            if (self->streamed(V0, V1, P)) return;
+        }
         if constexpr (kFloat) check(mclccd_traverse_f32(h_, V0, V1, nv_, P, mem_));
         else check(mclccd_traverse(h_, V0, V1, nv_, P, mem_));
         self->dispatch(V0, V1);
@@ -122,6 +126,9 @@ public:
     {
         auto *self = const_cast<BVHTree *>(this);
         self->push_options();
+        if constexpr (!kFloat) {
+            if (self->streamed(nullptr, nullptr, nullptr)) return;
+        }
         if constexpr (kFloat) check(mclccd_traverse_f32(h_, nullptr, nullptr, 0, nullptr, mem_));
         else check(mclccd_traverse(h_, nullptr, nullptr, 0, nullptr, mem_));
         self->dispatch(nullptr, nullptr);
@@ -234,6 +241,48 @@ private:
 #endif
     mclccd_tree *h_ = nullptr;
     int nv_ = 0, np_ = 0, mem_ = MCLCCD_MEM_HOST;
+    // hit staging for streamed(), kept across calls (capacity from the last count)
+    std::unique_ptr<int[]> out_s_;
+    std::unique_ptr<unsigned char[]> out_v_;
+    std::unique_ptr<double[]> out_t_;
+    long long out_cap_ = 0;
+
+    // With only append_pair / append_discrete set: traverse with the hits
+    // delivered into host staging (mclccd_traverse_out), so their copy from
+    // the device overlaps the rest of the step, then call the hooks.  The
+    // staging holds the previous call's count and a quarter more; hits beyond
+    // it are fetched after the step.  Returns false when hooks need the
+    // general path.
+    bool streamed(const double *V0, const double *V1, const int *P)
+    {
+        if (!append_pair || filter_pair || narrow_phase) return false;
+        long long nh = 0, nd = 0;
+        check(mclccd_traverse_out(h_, V0, V1, nv_, P, mem_, out_s_.get(), out_v_.get(), out_t_.get(), out_cap_, &nh,
+                                  nullptr, 0, &nd, MCLCCD_MEM_HOST));
+        if (nh > out_cap_) {
+            const long long cap = nh + nh / 4 + 1024;
+            std::unique_ptr<int[]> s(new int[4 * cap]);
+            std::unique_ptr<unsigned char[]> v(new unsigned char[cap]);
+            std::unique_ptr<double[]> t(new double[cap]);
+            check(mclccd_get_hits(h_, MCLCCD_MEM_HOST, nh, s.get(), v.get(), t.get()));
+            out_s_ = std::move(s);
+            out_v_ = std::move(v);
+            out_t_ = std::move(t);
+            out_cap_ = cap;
+        }
+        for (long long i = 0; i < nh; ++i) append_pair(make_stencil(&out_s_[4 * i]), out_v_[i] != 0, to_toi(out_t_[i]));
+        dispatch_discrete();
+        return true;
+    }
+    void dispatch_discrete()
+    {
+        if (append_discrete && options.discrete) {
+            std::vector<int> d;
+            discrete(d);
+            for (size_t i = 0; i < d.size() / 2; ++i)
+                if (append_discrete(d[2 * i], d[2 * i + 1])) break;
+        }
+    }
 
     void check(int rc) const
     {
@@ -326,12 +375,7 @@ private:
             hits(s, v, t);
             for (size_t i = 0; i < v.size(); ++i) append_pair(make_stencil(&s[4 * i]), v[i] != 0, to_toi(t[i]));
         }
-        if (append_discrete && options.discrete) {
-            std::vector<int> d;
-            discrete(d);
-            for (size_t i = 0; i < d.size() / 2; ++i)
-                if (append_discrete(d[2 * i], d[2 * i + 1])) break;
-        }
+        dispatch_discrete();
     }
 };
 

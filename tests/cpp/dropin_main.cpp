@@ -77,6 +77,9 @@ int main(int argc, char **argv)
     try {
         tree.update(V0.data(), V1.data(), F.data(), np, 3);
         tree.traverse(V0.data(), V1.data(), F.data());
+        // again: the hits now stream into the staging sized by the first call
+        hs.clear(); hv.clear(); ht.clear(); ds.clear();
+        tree.traverse(V0.data(), V1.data(), F.data());
     } catch (const mcl::CCDError &e) {
         std::fprintf(stderr, "CCDError %d: %s\n", e.status, e.what());
         return 1;
