@@ -294,7 +294,7 @@ struct HostOut {
 // while the next chunks compute.  The host waits on each chunk's event to
 // learn its hit count (a pinned snapshot).  Copies stop at the caller's
 // capacity; an overflow retry recomputes and copies again from the start.
-constexpr int kOutChunks = 8;
+constexpr int kOutChunks = 16;
 
 template <typename Accd>
 static int enqueue_streamed(mclccd_tree *t, int dim, int np, int nv, const int *dP, const double *dV1, bool discr,
