@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from mclccd_b200 import BVHTree, CCDError, narrow_phase_bulk, scenes
+from mclccd_b200 import PREC_FP64, BVHTree, CCDError, narrow_phase_bulk, scenes
 from oracle.ref import Port, canonical_set, sort_rows
 
 pytestmark = pytest.mark.gpu
@@ -120,6 +120,32 @@ def test_traverse_out_delivers_the_results(port):
     assert nh3 == n
     got = hit_map(hs[:small].numpy(), hv[:small].numpy(), ht[:small].numpy())
     assert len(got) == small and all(want[k] == v for k, v in got.items())
+
+
+@pytest.mark.parametrize("case", ["small", "certified", "2d"])
+def test_traverse_out_other_paths(case):
+    # delivery after the step instead of streaming (a scene below the
+    # chunking threshold, the certified form) and streaming in a 2D tree
+    torch = pytest.importorskip("torch")
+    from mclccd_b200 import PREC_FP32_CERTIFIED
+    V0, V1, F, eta = {"small": lambda: scenes.folded_cloth(20, seed=3),
+                      "certified": lambda: scenes.wavy_cloth(1025, rows=65, seed=4),
+                      "2d": lambda: scenes.annulus_2d(900, seed=5)}[case]()
+    t = BVHTree(V0.shape[1], precision=PREC_FP32_CERTIFIED if case == "certified" else PREC_FP64)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.update(V0, V1, F)
+    t.traverse()
+    want = hit_map(*t.hits())
+    wd = sort_rows(t.discrete())
+    cap = len(want) + 16
+    hs = torch.empty((cap, 4), dtype=torch.int32).pin_memory()
+    hv = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    ht = torch.empty(cap, dtype=torch.float64).pin_memory()
+    hd = torch.empty((len(wd) + 16, 2), dtype=torch.int32).pin_memory()
+    nh, nd = t.traverse_out(hs, hv, ht, hd)
+    assert (nh, nd) == (len(want), len(wd))
+    assert hit_map(hs[:nh].numpy(), hv[:nh].numpy(), ht[:nh].numpy()) == want
+    assert np.array_equal(sort_rows(hd[:nd].numpy()), wd)
 
 
 @pytest.mark.parametrize("chunks", [2, 5])
