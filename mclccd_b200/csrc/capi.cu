@@ -841,6 +841,10 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
         // A hit is a candidate: this capacity never overflows on its own.
         t->cap_hits = std::max(t->cap_hits, t->cap_vf + t->cap_ee);
         if (!grow) break;
+        // a retry regrows and rewrites the device lists: let copies of this
+        // attempt's hits (streamed results) finish first
+        if (t->s_copy) MC_CUDA(t, cudaStreamSynchronize(t->s_copy));
+        t->out_done = 0;
         if (attempt + 1 >= kMaxAttempts) return fail(t, MCLCCD_ERR_DEVICE, "result buffers kept overflowing");
     }
     const Counters &c = *t->h_cnt;

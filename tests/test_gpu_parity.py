@@ -122,6 +122,27 @@ def test_traverse_out_delivers_the_results(port):
     assert len(got) == small and all(want[k] == v for k, v in got.items())
 
 
+def test_traverse_out_overflow_retry(port):
+    # a fresh handle's lists are sized for a few stencils per triangle; the
+    # 64 x 64 fold has ~100 VF stencils per triangle, so the streamed step
+    # overflows, regrows and runs again: the delivered results are exact
+    torch = pytest.importorskip("torch")
+    V0, V1, F, eta = scenes.folded_cloth(64)
+    t = BVHTree(3)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.update(V0, V1, F)
+    cap = 2_500_000
+    hs = torch.empty((cap, 4), dtype=torch.int32).pin_memory()
+    hv = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    ht = torch.empty(cap, dtype=torch.float64).pin_memory()
+    hd = torch.empty((2048, 2), dtype=torch.int32).pin_memory()
+    nh, nd = t.traverse_out(hs, hv, ht, hd)
+    assert (nh, nd) == (2410926, 1061)
+    p = check_against_port(t, port, V0, V1, F, eta)
+    assert hit_map(hs[:nh].numpy(), hv[:nh].numpy(), ht[:nh].numpy()) == hit_map(*t.hits())
+    assert np.array_equal(sort_rows(hd[:nd].numpy()), sort_rows(p["discrete"]))
+
+
 @pytest.mark.parametrize("case", ["small", "certified", "2d"])
 def test_traverse_out_other_paths(case):
     # delivery after the step instead of streaming (a scene below the
