@@ -124,7 +124,7 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-# Algorithmic work per unit (also stated in DESIGN.md).
+# Algorithmic work per unit (the frozen per-unit formulas of the roofline).
 #   walk   : per query leaf its FP64 box (96 B) + prim id (4) + active (1), the
 #            n-1 internal nodes once (64 B), and per leaf pair found the
 #            candidate leaf box (96 B) + its prim id (4) + the pair write (8).

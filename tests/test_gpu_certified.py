@@ -1,6 +1,6 @@
 """FP32-certified form against the FP64 path.
 
-Bar (north star): identical hit/miss; the reported toi is never later than
+The bar: identical hit/miss; the reported toi is never later than
 the FP64 toi and within 1e-6 relative of it (toi 0 stays exactly 0);
 candidate and discrete sets unchanged."""
 import numpy as np
