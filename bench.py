@@ -339,7 +339,7 @@ def run_b200(args, rank, world, local):
             "traffic_source": "ncu dram bytes per unit (profiles/dram_traffic_per_unit.txt) x this run's units",
             "algorithmic_bytes": ab[top], "kernel_ms": kt[top],
             "note": "narrow = the VF and EE ACCD launches of one step; they are FP64-pipe bound "
-                    "(49-54% of peak in profiles/walk_expand_accd_wavy385.md), their vertex gathers hit L2",
+                    "(49-54% of peak in the committed ncu summary of these kernels), their vertex gathers hit L2",
             "all": {k: {"ms": kt[k], "GB/s": ab[k] / (kt[k] / 1e3) / 1e9 if kt[k] > 0 else None,
                         "traffic": tr.get(k)} for k in kt}}
 
