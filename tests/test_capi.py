@@ -53,3 +53,24 @@ def test_python_mirror_fails_loudly_without_library(monkeypatch, tmp_path):
     monkeypatch.setattr(ccd, "LIB_PATH", str(tmp_path / "missing.so"))
     with pytest.raises(ImportError):
         ccd.lib()
+
+
+def test_argument_checks_need_no_gpu():
+    # entry points reject a null handle or invalid arguments with a status
+    # before touching the device
+    L = ctypes.CDLL(LIB)
+    vp, ll = ctypes.c_void_p, ctypes.c_longlong
+    null = vp(0)
+    assert L.mclccd_traverse_out(null, null, null, 0, null, 0, null, null, null, ll(0), null, null, ll(0), null, 0) == 1
+    assert L.mclccd_update_ex(null, null, null, 0, null, 0, 3, null, 0, ctypes.c_uint(0)) == 1
+    assert L.mclccd_traverse_ex(null, null, null, 0, null, 0, ctypes.c_uint(0)) == 1
+    assert L.mclccd_batch_set_tuning(null, 0, 128) == 1
+    assert L.mclccd_batch_wave_stats(null, null, null) == 1
+    # one-sided VF with the certified form in the bulk call: unsupported
+    prec_cert, one_sided = 1, 0x100
+    rc = L.mclccd_narrow_phase_bulk_ex(3, null, null, 0, null, null, ll(1), ctypes.c_double(1e-3),
+                                       ctypes.c_double(1e-3), null, null, 0, null, prec_cert | one_sided, null)
+    assert rc == 7
+    rc = L.mclccd_narrow_phase_bulk_ex(5, null, null, 0, null, null, ll(1), ctypes.c_double(1e-3),
+                                       ctypes.c_double(1e-3), null, null, 0, null, 0, null)
+    assert rc == 1   # bad dim
