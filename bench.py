@@ -143,9 +143,10 @@ def algorithmic_bytes(c, n):
     return {"walk": walk, "expand": expand, "narrow": narrow, "refit": refit}
 
 
-def measured_traffic(c):
-    """DRAM bytes per stage of one step from the per-unit figures of the
-    committed ncu summary, scaled by this run's unit counts."""
+def per_unit_figures():
+    """The per-unit figures of the committed ncu summary
+    (profiles/dram_traffic_per_unit.txt): DRAM bytes per unit of each stage
+    and FP64 flops per VF / EE stencil of the narrow phase."""
     per = {}
     try:
         with open(os.path.join(ROOT, "profiles", "dram_traffic_per_unit.txt")) as f:
@@ -154,6 +155,33 @@ def measured_traffic(c):
                 if len(parts) == 2 and not line.startswith("#"):
                     per[parts[0]] = float(parts[1])
     except OSError:
+        return {}
+    return per
+
+
+# FP64 peak of a B200: 148 SMs x 64 FP64 FMA lanes x 2 flops at the 1965 MHz
+# maximum SM clock (no measured FP64 figure is available to divide by).
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+
+
+def fp64_roofline(c, narrow_ms, per=None):
+    """FP64 roofline of the narrow phase: the captured flops per VF and EE
+    stencil times this run's stencils, over the narrow stage's time."""
+    per = per_unit_figures() if per is None else per
+    if "narrow_fp64_flops_per_vf" not in per or not narrow_ms or narrow_ms <= 0:
+        return None
+    flops = per["narrow_fp64_flops_per_vf"] * c["vf"] + per.get("narrow_fp64_flops_per_ee", 0.0) * c["ee"]
+    achieved = flops / (narrow_ms / 1e3) / 1e12
+    return {"achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS,
+            "flops": flops, "peak_source": "nominal: 148 SMs x 64 FP64 FMA lanes x 2 flops x 1965 MHz",
+            "flops_source": "ncu thread-level DADD + DMUL + 2 DFMA per stencil, per kind"}
+
+
+def measured_traffic(c):
+    """DRAM bytes per stage of one step from the per-unit figures of the
+    committed ncu summary, scaled by this run's unit counts."""
+    per = per_unit_figures()
+    if not per:
         return {}
     out = {}
     sten = c["vf"] + c["ee"]
@@ -341,7 +369,8 @@ def run_b200(args, rank, world, local):
             "note": "narrow = the VF and EE ACCD launches of one step; they are FP64-pipe bound "
                     "(49-54% of peak in the committed ncu summary of these kernels), their vertex gathers hit L2",
             "all": {k: {"ms": kt[k], "GB/s": ab[k] / (kt[k] / 1e3) / 1e9 if kt[k] > 0 else None,
-                        "traffic": tr.get(k)} for k in kt}}
+                        "traffic": tr.get(k)} for k in kt},
+            "narrow_fp64": fp64_roofline(c, kt["narrow"])}
 
     # end to end through the C ABI from pinned host memory
     e2e = None

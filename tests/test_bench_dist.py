@@ -46,3 +46,18 @@ def test_single_rank_aggregate_is_local():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.aggregate(None, "cpu", 3.5, 7) == (3.5, 7.0)
+
+
+def test_fp64_roofline_of_the_narrow_phase():
+    # flops per stencil from the committed ncu summary x stencils / time,
+    # against 148 SMs x 64 FP64 lanes x 2 flops x 1965 MHz
+    import bench
+    per = bench.per_unit_figures()
+    assert per["narrow_fp64_flops_per_vf"] > 0 and per["narrow_fp64_flops_per_ee"] > 0
+    assert per["walk_bytes_per_leaf_pair"] > 0
+    c = {"vf": 1_000_000, "ee": 2_000_000}
+    r = bench.fp64_roofline(c, 1.0, per)
+    want = (per["narrow_fp64_flops_per_vf"] * 1e6 + per["narrow_fp64_flops_per_ee"] * 2e6) / 1e-3 / 1e12
+    assert abs(r["achieved"] - want) < 1e-9 and r["unit"] == "TFLOP/s"
+    assert abs(r["peak"] - 37.22) < 0.01 and abs(r["frac"] - want / r["peak"]) < 1e-12
+    assert bench.fp64_roofline(c, 0.0, per) is None and bench.fp64_roofline(c, 1.0, {}) is None
