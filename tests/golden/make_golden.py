@@ -12,7 +12,8 @@ left/right order comes from its Kd-tree); hit/toi of every candidate is also
 stored for the canonical orientation (lower primitive index first), by
 calling the reference's NarrowPhaseACCD::query_ccd_* on it directly.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # everything
+    python tests/golden/make_golden.py ctcd     # only kat_ctcd.npz (one-sided VF)
 """
 from __future__ import annotations
 
@@ -131,5 +132,44 @@ def main():
     print(json.dumps(summary, indent=1))
 
 
+def vf_stencils(rng, n, dim, coplanar=False):
+    """n VF stencils: a point near a triangle (an edge in 2D), all moving; with
+    coplanar, every start position in z = 0 (exact zero coefficients)."""
+    k = dim + 1
+    base = rng.uniform(0, 1, (n, 1, dim))
+    face = base + rng.normal(0, 0.1, (n, dim, dim))
+    w = rng.dirichlet(np.ones(dim), n)[:, :, None]
+    pt = (w * face).sum(1, keepdims=True) + rng.normal(0, 0.03, (n, 1, dim))
+    x0 = np.concatenate([pt, face], axis=1)
+    x1 = x0 + rng.normal(0, 0.05, (n, k, dim))
+    if coplanar:
+        x0[..., -1] = 0.0
+    sten = np.arange(n * k, dtype=np.int32).reshape(n, k)
+    if dim == 2:
+        sten = np.concatenate([sten, -np.ones((n, 1), np.int32)], axis=1)
+    return x0.reshape(-1, dim), x1.reshape(-1, dim), sten
+
+
+def ctcd_fixture():
+    """kat_ctcd.npz: the reference's one-sided VF narrow phase
+    (NarrowPhaseCTCD::query_ccd_vf with the wrong-side test) on seeded
+    stencils: its return code (1 hit, 0 none, -1 wrong side only) and toi."""
+    R = Reference()
+    arrays, eta = {}, 1e-3
+    for name, dim, coplanar, seed in (("vf3", 3, False, 101), ("vf3_coplanar", 3, True, 102), ("vf2", 2, False, 103)):
+        V0, V1, sten = vf_stencils(np.random.default_rng(seed), 1500, dim, coplanar)
+        ret, toi = R.ctcd_vf(V0, V1, sten, eta)
+        arrays.update({f"{name}/V0": V0, f"{name}/V1": V1, f"{name}/sten": sten, f"{name}/ret": ret,
+                       f"{name}/toi": toi})
+        print(f"{name}: {int((ret == 1).sum())} hits, {int((ret == -1).sum())} wrong-side only")
+    arrays["names"] = np.array(["vf3", "vf3_coplanar", "vf2"])
+    arrays["eta"] = np.array(eta)
+    np.savez_compressed(os.path.join(HERE, "kat_ctcd.npz"), **arrays)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["ctcd"]:
+        ctcd_fixture()
+    else:
+        main()
+        ctcd_fixture()

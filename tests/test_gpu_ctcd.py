@@ -171,3 +171,16 @@ def flat_slide(n):
     V1[right, 0] -= 0.3
     V1[right, 2] = 1e-4 * np.sin(37 * V0[right, 1])
     return V0, V1, F, eta
+
+
+def test_bulk_against_recorded_reference():
+    # the device one-sided narrow phase against the reference's recorded
+    # results (tests/golden/kat_ctcd.npz), with no reference build needed
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "kat_ctcd.npz"))
+    eta = float(z["eta"])
+    for name in z["names"]:
+        sten = z[f"{name}/sten"]
+        toi, hit = narrow_phase_bulk(z[f"{name}/V0"], z[f"{name}/V1"], sten, np.ones(len(sten), np.uint8), eta,
+                                     vf_one_sided=True)
+        compare(hit, toi, z[f"{name}/ret"], z[f"{name}/toi"], f"recorded {name}")

@@ -150,3 +150,14 @@ def test_reference_rpoly_matches_eigenvalue_roots():
             want = np.roots(op)
             assert len(got) == deg
             assert all(np.min(np.abs(want - g)) < 1e-8 for g in got), (got, want)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference oracle not built")
+def test_reference_reproduces_ctcd_fixture():
+    # kat_ctcd.npz holds the reference's one-sided VF results; the oracle
+    # build reproduces them bit for bit
+    z = np.load(os.path.join(GOLD, "kat_ctcd.npz"))
+    R = Reference()
+    for name in z["names"]:
+        ret, toi = R.ctcd_vf(z[f"{name}/V0"], z[f"{name}/V1"], z[f"{name}/sten"], float(z["eta"]))
+        assert np.array_equal(ret, z[f"{name}/ret"]) and np.array_equal(toi, z[f"{name}/toi"]), name
