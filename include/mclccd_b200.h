@@ -345,15 +345,22 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
  * shared memory, then walks the tree only for leaves beyond them; 0: tree
  * walk only), and overlap (K = 2..16: the queries in K chunks, the walk of
  * chunk c + 1 running while chunk c is expanded and scored, on two internal
- * streams; 0: in sequence; FP64 and one-sided forms only).  Results do not
- * depend on any of them. */
+ * streams; 0: in sequence; FP64 and one-sided forms only), the FP64 narrow
+ * phase form (1, the default: one kernel takes the leaf pairs to stencils,
+ * runs the discrete test and ACCD on them in per-warp batches of one kind,
+ * and counts the candidate lists without writing them (mclccd_get_candidates
+ * rebuilds them on request); 0: the expansion kernel writes the VF and EE
+ * lists and one ACCD kernel runs over each) and the grid size (in blocks) of
+ * that fused kernel.  Results do not depend on any of them. */
 #define MCLCCD_TUNE_EXPAND_GRID 0
 #define MCLCCD_TUNE_ACCD_GRID 1
 #define MCLCCD_TUNE_WALK_PACKET 2
 #define MCLCCD_TUNE_ACCD_REBIN 3
 #define MCLCCD_TUNE_WALK_WINDOW 4
 #define MCLCCD_TUNE_OVERLAP 5
-#define MCLCCD_TUNE_COUNT 6
+#define MCLCCD_TUNE_NARROW_FUSED 6
+#define MCLCCD_TUNE_FUSED_GRID 7
+#define MCLCCD_TUNE_COUNT 8
 int mclccd_set_tuning(mclccd_tree *tree, int key, int value);
 int mclccd_get_tuning(const mclccd_tree *tree, int key, int *value);
 

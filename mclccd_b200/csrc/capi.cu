@@ -24,6 +24,9 @@ struct DevBuf {
 // 16, 32} -> 2.43, 1.87, 1.81, 1.81 ms.
 constexpr int kExpandGrid = 148 * 16;
 constexpr int kAccdGrid = 148 * 128;
+// The fused pairs -> ACCD kernel is grid-stride over warp batches: one wave
+// of resident blocks (6 per SM).
+constexpr int kFusedGrid = 148 * 6;
 constexpr int kMaxAttempts = 6;
 
 struct DeviceGuard {
@@ -63,12 +66,13 @@ struct mclccd_tree {
     DevBuf nodes, leaf_parent, visits, leaf_box, leaf_active;
     DevBuf pairs, vf, ee, hit_sten, hit_toi, hit_isvf, disc, counters, diff, fp64_queue;
     DevBuf in_V, in_P, in_act, in_tmp;   // input conversion staging (mclccd_update_ex / mclccd_traverse_ex)
+    DevBuf cand_cnt;                     // counters of the on-request candidate expansion
     std::vector<DevBuf *> all()
     {
         return {&V0d, &V1d, &Pd, &Pstage, &actd, &pflags, &pflags_tmp, &vowner, &ekeys, &eowner, &cent, &bounds,
                 &keys, &vals, &keys_alt, &vals_alt, &sort_scratch, &nodes, &leaf_parent, &visits, &leaf_box,
                 &leaf_active, &pairs, &vf, &ee, &hit_sten, &hit_toi, &hit_isvf, &disc, &counters, &diff,
-                &fp64_queue, &in_V, &in_P, &in_act, &in_tmp};
+                &fp64_queue, &in_V, &in_P, &in_act, &in_tmp, &cand_cnt};
     }
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
@@ -84,7 +88,12 @@ struct mclccd_tree {
     cudaEvent_t out_ev[16] = {};
     unsigned long long *h_snap = nullptr;
     unsigned long long out_done = 0;   // hits already copied out by the streamed path
-    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0};
+    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0, 0, kFusedGrid};
+    // The fused narrow phase counts the candidate lists without writing them;
+    // mclccd_get_candidates rebuilds them from the leaf pairs and the P of the
+    // last traverse.
+    bool cand_lazy = false, cand_ready = false;
+    const int *tr_P = nullptr;
 };
 
 namespace {
@@ -232,8 +241,8 @@ static int stage_ints(mclccd_tree *t, DevBuf &buf, DevBuf &tmp, const int *src, 
 // range; the lists, hits and counts are the ones of the sequential order
 // (only their order in the buffers differs).
 template <typename Accd>
-static int enqueue_overlapped(mclccd_tree *t, int chunks, int dim, int np, int nv, const int *dP, const double *dV1,
-                              bool discr, Counters *cnt, Accd &accd)
+static int enqueue_overlapped(mclccd_tree *t, int chunks, int dim, int np, int nv, const int *dP, const double *dV0,
+                              const double *dV1, bool discr, bool fused, Counters *cnt, Accd &accd)
 {
     cudaStream_t st = t->stream;
     if (!t->s_walk) {
@@ -258,13 +267,21 @@ static int enqueue_overlapped(mclccd_tree *t, int chunks, int dim, int np, int n
         launch_snapshot(&cnt->n_pairs, pe + c + 1, nullptr, nullptr, t->s_walk);
         MC_CUDA(t, cudaEventRecord(t->ov_ev[1], t->s_walk));
         MC_CUDA(t, cudaStreamWaitEvent(t->s_narrow, t->ov_ev[1], 0));
-        launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
-                            as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc, 1,
-                            discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], t->s_narrow, pe + c, pe + c + 1);
-        launch_snapshot(&cnt->n_vf, ve + c + 1, &cnt->n_ee, ee + c + 1, t->s_narrow);
-        accd(true, t->vf, ve + c + 1, t->cap_vf, t->vf_eta, ve + c, t->s_narrow);
-        if (dim == 3) accd(false, t->ee, ee + c + 1, t->cap_ee, t->ee_eta, ee + c, t->s_narrow);
-        t->launches += 4;
+        if (fused) {
+            launch_narrow_fused(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV0, dV1, nv,
+                                t->vf_eta, t->ee_eta, 1, discr, as<int2>(t->disc), t->cap_disc, as<int4>(t->hit_sten),
+                                as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
+                                t->tune[MCLCCD_TUNE_FUSED_GRID], t->s_narrow, pe + c, pe + c + 1);
+            t->launches += 2;
+        } else {
+            launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                                as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
+                                1, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], t->s_narrow, pe + c, pe + c + 1);
+            launch_snapshot(&cnt->n_vf, ve + c + 1, &cnt->n_ee, ee + c + 1, t->s_narrow);
+            accd(true, t->vf, ve + c + 1, t->cap_vf, t->vf_eta, ve + c, t->s_narrow);
+            if (dim == 3) accd(false, t->ee, ee + c + 1, t->cap_ee, t->ee_eta, ee + c, t->s_narrow);
+            t->launches += 4;
+        }
     }
     MC_CUDA(t, cudaEventRecord(t->ov_ev[2], t->s_walk));   // join
     MC_CUDA(t, cudaEventRecord(t->ov_ev[3], t->s_narrow));
@@ -297,8 +314,8 @@ struct HostOut {
 constexpr int kOutChunks = 16;
 
 template <typename Accd>
-static int enqueue_streamed(mclccd_tree *t, int dim, int np, int nv, const int *dP, const double *dV1, bool discr,
-                            Counters *cnt, Accd &accd, const HostOut &out)
+static int enqueue_streamed(mclccd_tree *t, int dim, int np, int nv, const int *dP, const double *dV0,
+                            const double *dV1, bool discr, bool fused, Counters *cnt, Accd &accd, const HostOut &out)
 {
     cudaStream_t st = t->stream;
     if (!t->s_copy) {
@@ -316,13 +333,21 @@ static int enqueue_streamed(mclccd_tree *t, int dim, int np, int nv, const int *
                         as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
                         cnt, st, qb, qe);
         launch_snapshot(&cnt->n_pairs, pe + c + 1, nullptr, nullptr, st);
-        launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
-                            as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc, 1,
-                            discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st, pe + c, pe + c + 1);
-        launch_snapshot(&cnt->n_vf, ve + c + 1, &cnt->n_ee, ee + c + 1, st);
-        accd(true, t->vf, ve + c + 1, t->cap_vf, t->vf_eta, ve + c, st);
-        if (dim == 3) accd(false, t->ee, ee + c + 1, t->cap_ee, t->ee_eta, ee + c, st);
-        t->launches += 4;
+        if (fused) {
+            launch_narrow_fused(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV0, dV1, nv,
+                                t->vf_eta, t->ee_eta, 1, discr, as<int2>(t->disc), t->cap_disc, as<int4>(t->hit_sten),
+                                as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
+                                t->tune[MCLCCD_TUNE_FUSED_GRID], st, pe + c, pe + c + 1);
+            t->launches += 3;
+        } else {
+            launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                                as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
+                                1, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st, pe + c, pe + c + 1);
+            launch_snapshot(&cnt->n_vf, ve + c + 1, &cnt->n_ee, ee + c + 1, st);
+            accd(true, t->vf, ve + c + 1, t->cap_vf, t->vf_eta, ve + c, st);
+            if (dim == 3) accd(false, t->ee, ee + c + 1, t->cap_ee, t->ee_eta, ee + c, st);
+            t->launches += 4;
+        }
         MC_CUDA(t, cudaMemcpyAsync(t->h_snap + c, &cnt->n_hits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         MC_CUDA(t, cudaEventRecord(t->out_ev[c], st));
     }
@@ -767,18 +792,26 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
         t->cap_disc = std::max<unsigned long long>(1024, np / 4);
     }
     Counters *cnt = as<Counters>(t->counters);
+    const bool one_sided = (t->flags & MCLCCD_OPT_VF_ONE_SIDED) != 0;
+    const bool certified = t->precision == MCLCCD_PREC_FP32_CERTIFIED;
+    // FP64 ACCD on both kinds: the fused kernel unless the list form is asked for
+    const bool fused = cont && !one_sided && !certified && !t->tune[MCLCCD_TUNE_ACCD_REBIN] &&
+                       t->tune[MCLCCD_TUNE_NARROW_FUSED] != 0;
+    t->cand_lazy = fused;
+    t->cand_ready = false;
+    t->tr_P = dP;
     for (int attempt = 0;; ++attempt) {
         MC_CUDA(t, ensure(t->pairs, sizeof(int2) * t->cap_pairs));
-        MC_CUDA(t, ensure(t->vf, sizeof(int4) * t->cap_vf));
-        MC_CUDA(t, ensure(t->ee, sizeof(int4) * t->cap_ee));
+        if (!fused) {
+            MC_CUDA(t, ensure(t->vf, sizeof(int4) * t->cap_vf));
+            MC_CUDA(t, ensure(t->ee, sizeof(int4) * t->cap_ee));
+        }
         MC_CUDA(t, ensure(t->hit_sten, sizeof(int4) * t->cap_hits));
         MC_CUDA(t, ensure(t->hit_toi, sizeof(double) * t->cap_hits));
         MC_CUDA(t, ensure(t->hit_isvf, t->cap_hits));
         MC_CUDA(t, ensure(t->disc, sizeof(int2) * t->cap_disc));
-        const bool certified = t->precision == MCLCCD_PREC_FP32_CERTIFIED;
         if (certified && cont) MC_CUDA(t, ensure(t->fp64_queue, sizeof(unsigned) * std::max(t->cap_vf, t->cap_ee)));
         MC_CUDA(t, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
-        const bool one_sided = (t->flags & MCLCCD_OPT_VF_ONE_SIDED) != 0;
         // narrow phase of one list, stencils [*lo, *n) (lo == nullptr: from 0)
         auto accd = [&](bool vf, DevBuf &list, const unsigned long long *n_ptr, unsigned long long cap, double eta,
                         const unsigned long long *lo, cudaStream_t s) {
@@ -804,22 +837,31 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
         const bool stream_out = out && out->mem_kind == MCLCCD_MEM_HOST && cont && !certified &&
                                 !t->tune[MCLCCD_TUNE_WALK_PACKET] && np > 2 * kOutChunks * 128;
         if (stream_out) {
-            if (int rc = enqueue_streamed(t, dim, np, nv, dP, dV1, discr, cnt, accd, *out)) return rc;
+            if (int rc = enqueue_streamed(t, dim, np, nv, dP, dV0, dV1, discr, fused, cnt, accd, *out)) return rc;
         } else if (chunks >= 2 && cont && !certified && !t->tune[MCLCCD_TUNE_WALK_PACKET] && np > 2 * chunks * 128) {
-            if (int rc = enqueue_overlapped(t, chunks, dim, np, nv, dP, dV1, discr, cnt, accd)) return rc;
+            if (int rc = enqueue_overlapped(t, chunks, dim, np, nv, dP, dV0, dV1, discr, fused, cnt, accd)) return rc;
         } else {
             launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], t->tune[MCLCCD_TUNE_WALK_WINDOW],
                             as<Node>(t->nodes), t->leaf_box.p, as<unsigned char>(t->leaf_active), as<int>(t->vals), np,
                             as<int2>(t->pairs), t->cap_pairs, cnt, st);
             if (prof) cudaEventRecord(t->ev[4], st);
-            launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
-                                as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc),
-                                t->cap_disc, cont, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st);
-            if (prof) cudaEventRecord(t->ev[5], st);
-            t->launches += 2;
-            if (cont) {
-                accd(true, t->vf, &cnt->n_vf, t->cap_vf, t->vf_eta, nullptr, st);
-                if (dim == 3) accd(false, t->ee, &cnt->n_ee, t->cap_ee, t->ee_eta, nullptr, st);
+            if (fused) {   // expansion, discrete test and ACCD in one kernel: "expand" reads 0
+                if (prof) cudaEventRecord(t->ev[5], st);
+                launch_narrow_fused(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV0, dV1,
+                                    nv, t->vf_eta, t->ee_eta, 1, discr, as<int2>(t->disc), t->cap_disc,
+                                    as<int4>(t->hit_sten), as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf),
+                                    t->cap_hits, cnt, t->tune[MCLCCD_TUNE_FUSED_GRID], st);
+                t->launches += 2;
+            } else {
+                launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                                    as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc),
+                                    t->cap_disc, cont, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st);
+                if (prof) cudaEventRecord(t->ev[5], st);
+                t->launches += 2;
+                if (cont) {
+                    accd(true, t->vf, &cnt->n_vf, t->cap_vf, t->vf_eta, nullptr, st);
+                    if (dim == 3) accd(false, t->ee, &cnt->n_ee, t->cap_ee, t->ee_eta, nullptr, st);
+                }
             }
         }
         if (prof) cudaEventRecord(t->ev[6], st);
@@ -835,11 +877,15 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
         // them by the leaf-pair shortfall so one regrow usually suffices.
         const double r = c.n_pairs > t->cap_pairs ? (double)c.n_pairs / (double)t->cap_pairs : 1.0;
         need((double)c.n_pairs, t->cap_pairs);
-        need(r * (double)c.n_vf, t->cap_vf);
-        need(r * (double)c.n_ee, t->cap_ee);
         need(r * (double)c.n_discrete, t->cap_disc);
-        // A hit is a candidate: this capacity never overflows on its own.
-        t->cap_hits = std::max(t->cap_hits, t->cap_vf + t->cap_ee);
+        if (fused) {   // no candidate lists: only the hits need room
+            need(r * (double)c.n_hits, t->cap_hits);
+        } else {
+            need(r * (double)c.n_vf, t->cap_vf);
+            need(r * (double)c.n_ee, t->cap_ee);
+            // A hit is a candidate: this capacity never overflows on its own.
+            t->cap_hits = std::max(t->cap_hits, t->cap_vf + t->cap_ee);
+        }
         if (!grow) break;
         // a retry regrows and rewrites the device lists: let copies of this
         // attempt's hits (streamed results) finish first
@@ -945,6 +991,25 @@ int mclccd_get_candidates(mclccd_tree *t, int mem_kind, long long capacity, int 
     if (!t->traversed) return fail(t, MCLCCD_ERR_STATE, "no traverse results");
     if (capacity < 0 || (mem_kind != MCLCCD_MEM_HOST && mem_kind != MCLCCD_MEM_DEVICE)) return MCLCCD_ERR_INVALID;
     DeviceGuard g(t->device);
+    if (t->cand_lazy && !t->cand_ready && sten) {
+        // The fused narrow phase only counted the candidates: expand the leaf
+        // pairs of the last traverse again (same kernel, same P and flags),
+        // into lists sized by those counts.
+        t->cap_vf = std::max<unsigned long long>(t->cap_vf, t->n_vf);
+        t->cap_ee = std::max<unsigned long long>(t->cap_ee, t->n_ee);
+        MC_CUDA(t, ensure(t->vf, sizeof(int4) * t->cap_vf));
+        MC_CUDA(t, ensure(t->ee, sizeof(int4) * t->cap_ee));
+        MC_CUDA(t, ensure(t->cand_cnt, sizeof(Counters)));
+        Counters *cc = as<Counters>(t->cand_cnt);
+        MC_CUDA(t, cudaMemsetAsync(cc, 0, sizeof(Counters), t->stream));
+        launch_expand_pairs(t->dim, as<int2>(t->pairs), t->cap_pairs, t->tr_P, as<unsigned char>(t->pflags), t->tr_V1,
+                            t->tr_nv, as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, nullptr, 0, 1, 0, cc,
+                            t->tune[MCLCCD_TUNE_EXPAND_GRID], t->stream, nullptr,
+                            &as<Counters>(t->counters)->n_pairs);
+        ++t->launches;
+        if (int rc = check_launch(t, "candidate expansion")) return rc;
+        t->cand_ready = true;
+    }
     const unsigned long long total = t->n_vf + t->n_ee;
     const size_t nvf = (size_t)std::min<unsigned long long>(t->n_vf, (unsigned long long)capacity);
     const size_t nee = (size_t)std::min<unsigned long long>(t->n_ee, (unsigned long long)capacity - nvf);
@@ -1220,7 +1285,7 @@ int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)
 int mclccd_set_tuning(mclccd_tree *t, int key, int value)
 {
     if (!t || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
-    const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_ACCD_REBIN;
+    const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_ACCD_REBIN || key == MCLCCD_TUNE_NARROW_FUSED;
     if (key == MCLCCD_TUNE_OVERLAP) {
         if (value < 0 || value > 16) return fail(t, MCLCCD_ERR_INVALID, "overlap chunks must be in [0, 16]");
     } else if (key == MCLCCD_TUNE_WALK_WINDOW) {

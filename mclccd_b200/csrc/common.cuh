@@ -4,6 +4,11 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+// Pure arithmetic shared by device kernels and the host-side tests.
+#ifndef MC_HD
+#define MC_HD __host__ __device__ __forceinline__
+#endif
+
 namespace mclccd {
 
 // ---------------------------------------------------------------------------

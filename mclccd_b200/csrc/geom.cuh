@@ -8,6 +8,8 @@
 
 #include "common.cuh"
 
+#include <cmath>
+
 namespace mclccd {
 
 // ---------------------------------------------------------------------------
@@ -40,50 +42,73 @@ __device__ __forceinline__ bool leaf_boxes_intersect(const LeafBox<DIM> &l, cons
 
 // ---------------------------------------------------------------------------
 // Distances (Projection.hpp).
+//
+// Each routine keeps the reference's case analysis and expressions, but the
+// quotient a case needs is selected first and divided once: every case of
+// point_on_triangle takes exactly one quotient (num / den), edge_to_edge at
+// most two.  The same IEEE operations run on the same operands, so the
+// results are the reference's bit for bit, while the lanes of a warp that
+// fall into different cases share one division instead of taking each
+// case's in turn.  Host-callable too, so the CPU tests can run this code.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double dot3(const double *a, const double *b)
+MC_HD double dot3(const double *a, const double *b)
 {
     return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
-__device__ __forceinline__ double clamp_zero_one(double v) { return v < 0 ? 0.0 : (v > 1 ? 1.0 : v); }
+MC_HD double clamp_zero_one(double v) { return v < 0 ? 0.0 : (v > 1 ? 1.0 : v); }
 // std::min(T(1), std::max(x, T(0))) as the reference writes it.
-__device__ __forceinline__ double clamp01(double x)
+MC_HD double clamp01(double x)
 {
     double m = x < 0 ? 0.0 : x;
     return m < 1 ? m : 1.0;
 }
 
 // Distance from pt to triangle (p1,p2,p3): point_on_triangle
-// (Projection.hpp:61-145) then (pt - closest).norm().
-__device__ __forceinline__ double vf_distance3(const double *pt, const double *p1, const double *p2, const double *p3)
+// (Projection.hpp:61-145) then (pt - closest).norm().  Cases, by the
+// quotient q = num / den they take:
+//   interior:               q = 1 / det,  s = s0 q, t = t0 q
+//   s = clamp(q), t = 0:    q = -d / a  (Projection.hpp region 4 / 5), or
+//                           q = -e / c  (the branch s >= 0, t < 0, s+t >= det,
+//                                        a+d <= b+e, which the reference
+//                                        writes as s = clamp(-e/c), t = 0)
+//   s = 0, t = clamp(q):    q = -e / c
+//   s = clamp(q), t = 1-s:  q = (c+e) - (b+d) over (a - 2b) + c  (region 2), or
+//                           q = ((c+e) - b) - d over the same   (regions 6, 1)
+MC_HD double vf_distance3(const double *pt, const double *p1, const double *p2, const double *p3)
 {
     double e0[3], e1[3], v0[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) { e0[k] = p2[k] - p1[k]; e1[k] = p3[k] - p1[k]; v0[k] = p1[k] - pt[k]; }
     const double a = dot3(e0, e0), b = dot3(e0, e1), c = dot3(e1, e1), d = dot3(e0, v0), e = dot3(e1, v0);
     const double det = a * c - b * b;
-    double s = b * e - c * d, t = b * d - a * e;
-    if (s + t < det) {
-        if (s < 0) {
-            if (t < 0) {
-                if (d < 0) { s = clamp_zero_one(-d / a); t = 0; }
-                else { s = 0; t = clamp_zero_one(-e / c); }
-            } else { s = 0; t = clamp_zero_one(-e / c); }
-        } else if (t < 0) { s = clamp_zero_one(-d / a); t = 0; }
-        else { const double inv = 1.0 / det; s *= inv; t *= inv; }
+    const double s0 = b * e - c * d, t0 = b * d - a * e;
+    enum { kInterior, kSOnly, kTOnly, kEdge12 };
+    double num, den;
+    int kind;
+    if (s0 + t0 < det) {
+        if (s0 < 0) {
+            if (t0 < 0 && d < 0) { num = -d; den = a; kind = kSOnly; }
+            else { num = -e; den = c; kind = kTOnly; }
+        } else if (t0 < 0) { num = -d; den = a; kind = kSOnly; }
+        else { num = 1.0; den = det; kind = kInterior; }
     } else {
-        if (s < 0) {
-            const double t0 = b + d, t1 = c + e;
-            if (t1 > t0) { s = clamp_zero_one((t1 - t0) / (a - 2.0 * b + c)); t = 1 - s; }
-            else { t = clamp_zero_one(-e / c); s = 0; }
-        } else if (t < 0) {
-            if (a + d > b + e) { s = clamp_zero_one((c + e - b - d) / (a - 2.0 * b + c)); t = 1 - s; }
-            else { s = clamp_zero_one(-e / c); t = 0; }
-        } else {
-            s = clamp_zero_one((c + e - b - d) / (a - 2.0 * b + c));
-            t = 1 - s;
-        }
+        const double den12 = a - 2.0 * b + c;
+        if (s0 < 0) {
+            const double tt0 = b + d, tt1 = c + e;
+            if (tt1 > tt0) { num = tt1 - tt0; den = den12; kind = kEdge12; }
+            else { num = -e; den = c; kind = kTOnly; }
+        } else if (t0 < 0) {
+            if (a + d > b + e) { num = c + e - b - d; den = den12; kind = kEdge12; }
+            else { num = -e; den = c; kind = kSOnly; }
+        } else { num = c + e - b - d; den = den12; kind = kEdge12; }
     }
+    const double q = num / den;
+    const double cq = clamp_zero_one(q);
+    double s, t;
+    if (kind == kInterior) { s = s0 * q; t = t0 * q; }
+    else if (kind == kSOnly) { s = cq; t = 0.0; }
+    else if (kind == kTOnly) { s = 0.0; t = cq; }
+    else { s = cq; t = 1 - cq; }
     double r[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) r[k] = pt[k] - ((p1[k] + e0[k] * s) + e1[k] * t);
@@ -91,7 +116,9 @@ __device__ __forceinline__ double vf_distance3(const double *pt, const double *p
 }
 
 // Segment-segment distance: edge_to_edge (Projection.hpp:242-302), .norm().
-__device__ __forceinline__ double ee_distance3(const double *p0, const double *p1, const double *q0, const double *q1)
+// First quotient s = clamp((bf - ce) / denom) (unused when denom == 0), then
+// one of -c / a, (b - c) / a (s re-clamped, t = 0 or 1) or t = tnom / e.
+MC_HD double ee_distance3(const double *p0, const double *p1, const double *q0, const double *q1)
 {
     double d1[3], d2[3], r[3];
 #pragma unroll
@@ -99,12 +126,17 @@ __device__ __forceinline__ double ee_distance3(const double *p0, const double *p
     const double a = dot3(d1, d1), e = dot3(d2, d2), f = dot3(d2, r);
     const double c = dot3(d1, r), b = dot3(d1, d2);
     const double denom = a * e - b * b;
-    double s = denom != 0 ? clamp01((b * f - c * e) / denom) : 0.0;
-    double t;
+    const double q1s = (b * f - c * e) / denom;
+    double s = denom != 0 ? clamp01(q1s) : 0.0;
     const double tnom = b * s + f;
-    if (tnom < 0 || e == 0) { t = 0; s = (a == 0) ? 0.0 : clamp01(-c / a); }
-    else if (tnom > e) { t = 1.0; s = (a == 0) ? 0.0 : clamp01((b - c) / a); }
-    else t = tnom / e;
+    double num, den, t;
+    int kind;   // 0: t = 0, 1: t = 1 (s from q), 2: t = q
+    if (tnom < 0 || e == 0) { num = -c; den = a; kind = 0; }
+    else if (tnom > e) { num = b - c; den = a; kind = 1; }
+    else { num = tnom; den = e; kind = 2; }
+    const double q = num / den;
+    if (kind == 2) t = q;
+    else { t = kind == 0 ? 0.0 : 1.0; s = (a == 0) ? 0.0 : clamp01(q); }
     double w[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) w[k] = (q0[k] + t * d2[k]) - (p0[k] + s * d1[k]);
@@ -112,25 +144,22 @@ __device__ __forceinline__ double ee_distance3(const double *p0, const double *p
 }
 
 // Point-segment distance in 2D: point_on_edge (Projection.hpp:194-204).
-__device__ __forceinline__ double vf_distance2(const double *p, const double *e0, const double *e1)
+MC_HD double vf_distance2(const double *p, const double *e0, const double *e1)
 {
     const double e[2] = {e1[0] - e0[0], e1[1] - e0[1]};
     const double len2 = e[0] * e[0] + e[1] * e[1];
+    const double t = ((p[0] - e0[0]) * e[0] + (p[1] - e0[1]) * e[1]) / len2;   // unused when len2 <= 0
     double q0, q1;
-    if (len2 <= 0.0) { q0 = e0[0]; q1 = e0[1]; }
-    else {
-        const double t = ((p[0] - e0[0]) * e[0] + (p[1] - e0[1]) * e[1]) / len2;
-        if (t < 0.0) { q0 = e0[0]; q1 = e0[1]; }
-        else if (t > 1.0) { q0 = e1[0]; q1 = e1[1]; }
-        else { q0 = e0[0] + t * e[0]; q1 = e0[1] + t * e[1]; }
-    }
+    if (len2 <= 0.0 || t < 0.0) { q0 = e0[0]; q1 = e0[1]; }
+    else if (t > 1.0) { q0 = e1[0]; q1 = e1[1]; }
+    else { q0 = e0[0] + t * e[0]; q1 = e0[1] + t * e[1]; }
     const double w0 = p[0] - q0, w1 = p[1] - q1;
     return sqrt(w0 * w0 + w1 * w1);
 }
 
 // NarrowPhaseACCD::pair_distance (NarrowPhase.cpp:714-750).
 template <int DIM, bool VF>
-__device__ __forceinline__ double pair_distance(const double (&x)[DIM + 1][DIM])
+MC_HD double pair_distance(const double (&x)[DIM + 1][DIM])
 {
     if constexpr (DIM == 2) return vf_distance2(x[0], x[1], x[2]);
     else if constexpr (VF) return vf_distance3(x[0], x[1], x[2], x[3]);
@@ -156,10 +185,13 @@ __device__ __forceinline__ double pair_distance(const double (&x)[DIM + 1][DIM])
 // when WANT_LP -- l_p = max first |p| + max second |p| (NarrowPhase.cpp:647-670).
 // step0_noop: x + 0 * p == x bit for bit (every p finite, no x is -0.0, the
 // only value whose bits change: -0.0 + 0.0 == +0.0).
+// l_p is formed from the squared norms: sqrt is correctly rounded and
+// monotone, so the larger of two square roots is the square root of the
+// larger square (ties and NaN behave the same), which takes two square
+// roots per stencil instead of DIM + 1.
 template <int DIM, bool VF, bool WANT_LP>
-__device__ __forceinline__ void accd_setup(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM],
-                                           double (&p)[DIM + 1][DIM], double (&x)[DIM + 1][DIM], double &l_p,
-                                           bool &step0_noop)
+MC_HD void accd_setup(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM],
+                      double (&p)[DIM + 1][DIM], double (&x)[DIM + 1][DIM], double &l_p, bool &step0_noop)
 {
     constexpr int ns = DIM + 1;
     double pbar[DIM];
@@ -175,7 +207,7 @@ __device__ __forceinline__ void accd_setup(const double (&v0)[DIM + 1][DIM], con
             x[i][k] = v0[i][k];
             pbar[k] = pbar[k] + w * p[i][k];
         }
-    double lf = 0.0, ls = 0.0;
+    double lf2 = 0.0, ls2 = 0.0;
 #pragma unroll
     for (int i = 0; i < ns; ++i) {
         double sq = 0.0;
@@ -186,20 +218,19 @@ __device__ __forceinline__ void accd_setup(const double (&v0)[DIM + 1][DIM], con
             step0_noop = step0_noop && isfinite(p[i][k]) && !(x[i][k] == 0.0 && signbit(x[i][k]));
         }
         if constexpr (WANT_LP) {
-            const double n = sqrt(sq);
             const bool first = VF ? (i == 0) : (i <= 1);
-            if (first) lf = lf < n ? n : lf;
-            else ls = ls < n ? n : ls;
+            if (first) lf2 = lf2 < sq ? sq : lf2;
+            else ls2 = ls2 < sq ? sq : ls2;
         }
     }
-    if constexpr (WANT_LP) l_p = lf + ls;
+    if constexpr (WANT_LP) l_p = sqrt(lf2) + sqrt(ls2);
 }
 
 // Iterations 1..999 of the reference loop, from the state after iteration 0
 // (positions x, accumulated toi, next step t_l, threshold g).
 template <int DIM, bool VF>
-__device__ __forceinline__ int accd_tail(double (&x)[DIM + 1][DIM], const double (&p)[DIM + 1][DIM], double l_p,
-                                         double xsi, double g, double &toi, double t_l, int &iters)
+MC_HD int accd_tail(double (&x)[DIM + 1][DIM], const double (&p)[DIM + 1][DIM], double l_p, double xsi, double g,
+                    double &toi, double t_l, int &iters)
 {
     constexpr int ns = DIM + 1;
     const double xx = xsi * xsi;
@@ -222,7 +253,7 @@ __device__ __forceinline__ int accd_tail(double (&x)[DIM + 1][DIM], const double
 }
 
 // Outcome of ACCD's head (everything before iteration 1).
-enum AccdHead { kHeadMiss = 0, kHeadHit = 1, kHeadContinue = 2 };
+enum AccdHead { kHeadMiss = 0, kHeadHit = 1, kHeadContinue = 2, kHeadLiteral = 3 };
 
 // Head: l_p test, first distance, immediate hit, iteration 0, and the miss
 // that iteration 1 would report before its distance is used.  On
@@ -230,9 +261,8 @@ enum AccdHead { kHeadMiss = 0, kHeadHit = 1, kHeadContinue = 2 };
 // the first distance.  exact_skip tells whether iteration 0 was skipped
 // (then x == v0, toi == 0 and t_l is a function of d0 and l_p alone).
 template <int DIM, bool VF>
-__device__ __forceinline__ int accd_head(double (&x)[DIM + 1][DIM], const double (&p)[DIM + 1][DIM], double l_p,
-                                         bool step0_noop, double xsi, double &d0, double &g, double &toi,
-                                         double &t_l, bool &exact_skip)
+MC_HD int accd_head(double (&x)[DIM + 1][DIM], const double (&p)[DIM + 1][DIM], double l_p, bool step0_noop,
+                    double xsi, double &d0, double &g, double &toi, double &t_l, bool &exact_skip)
 {
     constexpr int ns = DIM + 1;
     exact_skip = false;
@@ -261,9 +291,45 @@ __device__ __forceinline__ int accd_head(double (&x)[DIM + 1][DIM], const double
     return kHeadContinue;
 }
 
+// The same head with the work the outcome does not need left out: the
+// threshold g (used from iteration 2 on) is not formed, and iteration 0's
+// step ((1 - 1) A) / X is not divided out when it is certainly zero (A
+// finite, X neither zero nor NaN), which is exactly when the reference's
+// step is +-0.  Outcomes: kHeadMiss, kHeadHit (toi = 0), kHeadContinue (the
+// state entering iteration 1 is x = v0, toi = 0, t_l = t_l1, and g follows
+// from d0: accd_resume) or kHeadLiteral (iteration 0 is not an exact no-op:
+// run the literal accd).
 template <int DIM, bool VF>
-__device__ __forceinline__ int accd(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM],
-                                    double xsi, double &toi, int &iters)
+MC_HD int accd_head_fast(const double (&x)[DIM + 1][DIM], double l_p, bool step0_noop, double xsi, double &d0,
+                         double &t_l1)
+{
+    if (l_p <= 0) return kHeadMiss;
+    const double d = pair_distance<DIM, VF>(x);
+    d0 = d;
+    const double A = d * d - xsi * xsi;
+    const double X = (d + xsi) * l_p;
+    if (d <= xsi) return kHeadHit;
+    const bool zero_step = isfinite(A) && X == X && X != 0.0;
+    if (!(zero_step && step0_noop)) return kHeadLiteral;
+    t_l1 = 0.9 * A / X;
+    return t_l1 > 1.0 ? kHeadMiss : kHeadContinue;   // 0 + t_l1 > 1 at iteration 1
+}
+
+// Iterations 1.. for a stencil whose fast head said kHeadContinue: x holds
+// v0 and p the relative motion (accd_setup), d0 the first distance.
+template <int DIM, bool VF>
+MC_HD int accd_resume(double (&x)[DIM + 1][DIM], const double (&p)[DIM + 1][DIM], double l_p, double xsi, double d0,
+                      double &toi, int &iters)
+{
+    const double A = d0 * d0 - xsi * xsi;
+    const double g = (1.0 * A) / (d0 - xsi);
+    toi = 0.0;
+    return accd_tail<DIM, VF>(x, p, l_p, xsi, g, toi, 0.9 * A / ((d0 + xsi) * l_p), iters);
+}
+
+template <int DIM, bool VF>
+MC_HD int accd_literal(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM], double xsi, double &toi,
+                       int &iters)
 {
     constexpr int ns = DIM + 1;
     double p[ns][DIM], x[ns][DIM], l_p, d0, g, t_l;
@@ -274,6 +340,21 @@ __device__ __forceinline__ int accd(const double (&v0)[DIM + 1][DIM], const doub
     if (h == kHeadHit) { iters = 0; return 1; }
     if (h == kHeadMiss) { iters = l_p <= 0 ? -1 : 0; return 0; }
     return accd_tail<DIM, VF>(x, p, l_p, xsi, g, toi, t_l, iters);
+}
+
+template <int DIM, bool VF>
+MC_HD int accd(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM], double xsi, double &toi,
+               int &iters)
+{
+    constexpr int ns = DIM + 1;
+    double p[ns][DIM], x[ns][DIM], l_p, d0, t_l1;
+    bool noop;
+    accd_setup<DIM, VF, true>(v0, v1, p, x, l_p, noop);
+    const int h = accd_head_fast<DIM, VF>(x, l_p, noop, xsi, d0, t_l1);
+    if (h == kHeadHit) { toi = 0.0; iters = 0; return 1; }
+    if (h == kHeadMiss) { iters = l_p <= 0 ? -1 : 0; return 0; }
+    if (h == kHeadLiteral) return accd_literal<DIM, VF>(v0, v1, xsi, toi, iters);
+    return accd_resume<DIM, VF>(x, p, l_p, xsi, d0, toi, iters);
 }
 
 // ---------------------------------------------------------------------------

@@ -42,6 +42,14 @@ void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned lon
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
                           unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, bool rebin,
                           cudaStream_t st, const unsigned long long *lo_ptr = nullptr);
+// fused.cu: leaf pairs [*lo, *hi) -> stencils -> discrete test + FP64 ACCD in
+// one kernel (candidate lists counted, not written)
+void launch_narrow_fused(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,
+                         const unsigned char *flags, const double *V0, const double *V1, int nv, double vf_eta,
+                         double ee_eta, int continuous, int discrete, int2 *disc, unsigned long long disc_cap,
+                         int4 *hit_sten, double *hit_toi, unsigned char *hit_isvf, unsigned long long hit_cap,
+                         Counters *cnt, int grid, cudaStream_t st, const unsigned long long *lo_ptr = nullptr,
+                         const unsigned long long *hi_ptr = nullptr);
 // certified.cu
 void launch_accd_certified(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr,
                            unsigned long long cap, const double *V0, const double *V1, int nv, double eta,

@@ -6,6 +6,8 @@ row order, so full-size outputs can be compared without sorting.
 """
 import numpy as np
 
+from oracle.ref import canon_ee
+
 _M1 = np.uint64(0xBF58476D1CE4E5B9)
 _M2 = np.uint64(0x94D049BB133111EB)
 
@@ -35,3 +37,24 @@ def set_digest(rows):
         s = int(np.sum(h, dtype=np.uint64))
     x = int(np.bitwise_xor.reduce(h)) if len(h) else 0
     return [int(len(h)), s, x]
+
+
+def set_rows(sten, is_vf):
+    """(is_vf, s0..s3) int64 rows of a stencil set, EE stencils in
+    lexicographic orientation ([a,b,c,d] vs [c,d,a,b]: the smaller)."""
+    s = np.asarray(sten, np.int64).reshape(-1, 4).copy()
+    v = np.asarray(is_vf).astype(np.int64).reshape(-1)
+    ee = v == 0
+    if ee.any():
+        s[ee] = canon_ee(s[ee])
+    return np.concatenate([v[:, None], s], axis=1)
+
+
+def hit_rows(sten, is_vf, toi):
+    """(is_vf, s0..s3, toi bits) rows: a hit and its exact toi, in the
+    orientation given (lower primitive index first for EE stencils, as the
+    device emits them and the oracle restatement enumerates them)."""
+    s = np.asarray(sten, np.int64).reshape(-1, 4)
+    v = np.asarray(is_vf).astype(np.int64).reshape(-1, 1)
+    t = np.ascontiguousarray(toi, np.float64).view(np.int64).reshape(-1, 1)
+    return np.concatenate([v, s, t], axis=1)

@@ -14,6 +14,7 @@ calling the reference's NarrowPhaseACCD::query_ccd_* on it directly.
 
     python tests/golden/make_golden.py          # everything
     python tests/golden/make_golden.py ctcd     # only kat_ctcd.npz (one-sided VF)
+    python tests/golden/make_golden.py cfg1     # only cfg1_digests.json (2.1M-triangle cloth)
 """
 from __future__ import annotations
 
@@ -30,6 +31,7 @@ sys.path.insert(0, ROOT)
 
 from mclccd_b200 import scenes  # noqa: E402
 from oracle.ref import Port, Reference, canonical_set, sort_rows  # noqa: E402
+sys.path.insert(0, os.path.dirname(HERE))
 
 
 def digest(a: np.ndarray) -> str:
@@ -167,9 +169,58 @@ def ctcd_fixture():
     np.savez_compressed(os.path.join(HERE, "kat_ctcd.npz"), **arrays)
 
 
+def cfg1_digests():
+    """cfg1_digests.json: the full 2,097,152-triangle wavy cloth (1025 x 1025
+    grid, thickness 1e-4) for both V1 draws of the timed step (seed 0, then the
+    redraw with seed 1 over the same F, which the device takes through its
+    refit-only path).  Per draw, order-independent digests (tests/digest.py)
+    of the reference's candidate set (filter_pair), discrete-pair set
+    (append_discrete) and hit set (append_pair), and of the hit/toi map in
+    the device's orientation: the reference's own NarrowPhaseACCD::query_ccd_*
+    called on every candidate in that orientation (the oracle restatement
+    supplies the orientation; its candidate and hit sets are checked equal to
+    the reference's first)."""
+    import time
+    from digest import hit_rows, set_digest, set_rows
+    R, P = Reference(), Port()
+    V0, V1a, F, eta = scenes.wavy_cloth(1025, seed=0)
+    V1b = scenes.wavy_redraw(V0, 1)
+    out = {"scene": "wavy_cloth(1025, seed=0); draw b = wavy_redraw(V0, 1)", "eta": eta, "tris": int(len(F)),
+           "F_sha256": hashlib.sha256(F.tobytes()).hexdigest(),
+           "V0_sha256": hashlib.sha256(V0.tobytes()).hexdigest(), "draws": {}}
+    for name, V1 in (("a", V1a), ("b", V1b)):
+        t0 = time.time()
+        r = R.run(V0, V1, F, eta)
+        ref_cand = set_digest(set_rows(r["cand_sten"], r["cand_is_vf"]))
+        ref_hits = set_digest(set_rows(r["hit_sten"], r["hit_is_vf"]))
+        ref_disc = set_digest(np.sort(r["discrete"], axis=1))
+        del r
+        t1 = time.time()
+        p = P.run(V0, V1, F, eta)
+        assert set_digest(set_rows(p["cand_sten"], p["cand_is_vf"])) == ref_cand
+        assert set_digest(set_rows(p["hit_sten"], p["hit_is_vf"])) == ref_hits
+        assert set_digest(np.asarray(p["discrete"])) == ref_disc
+        hit, toi = R.accd(V0, V1, p["cand_sten"], p["cand_is_vf"], eta)
+        m = (hit == 1) & (toi >= 0)   # collide() delivers only toi >= 0 (BVHTree.cpp:262)
+        toi_map = set_digest(hit_rows(p["cand_sten"][m], p["cand_is_vf"][m], toi[m]))
+        out["draws"][name] = {
+            "V1_sha256": hashlib.sha256(V1.tobytes()).hexdigest(),
+            "n_leaf_pairs": int(len(p["leaf_pairs"])),
+            "n_vf": int(p["cand_is_vf"].sum()), "n_ee": int(len(p["cand_is_vf"]) - p["cand_is_vf"].sum()),
+            "candidates": ref_cand, "hits": ref_hits, "discrete": ref_disc, "hit_toi": toi_map}
+        print(f"draw {name}: reference {t1 - t0:.0f} s, oracle + reference ACCD {time.time() - t1:.0f} s: "
+              f"{ref_cand[0]} candidates, {ref_hits[0]} hits, {ref_disc[0]} discrete", flush=True)
+        del p, hit, toi
+    with open(os.path.join(HERE, "cfg1_digests.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["ctcd"]:
         ctcd_fixture()
+    elif sys.argv[1:] == ["cfg1"]:
+        cfg1_digests()
     else:
         main()
         ctcd_fixture()
+        cfg1_digests()
