@@ -14,7 +14,8 @@ whole job with inputs resident in HBM; e2e = the same through the C ABI from
 pinned host buffers, host<->device copies of inputs and of every hit and
 discrete pair inside the timed region.  --impl reference times the
 reference's own CPU code (the oracle build of the unmodified reference
-sources) on the host cores, on a 257-row strip of the same cloth per step.
+sources) on the host cores, on the same full cloth and the same step
+(second update with the same F, then traverse), K timed steps after W.
 """
 from __future__ import annotations
 
@@ -133,29 +134,37 @@ class Clocks:
 #            6 V1 vertices (144 B) per pair.
 #   narrow : per stencil 16 B read + 2 x 4 x 24 B vertex gather (192 B), plus
 #            25 B per hit written (int4 stencil, f64 toi, u8 kind).
+#   fused  : (expansion, discrete test and ACCD in one kernel, no stencil
+#            lists) per leaf pair 8 + 26 + 144 B, 8 B per discrete pair, per
+#            stencil the 192 B vertex gather, 25 B per hit.
 #   refit  : per leaf 12 B face + 6 x 24 B vertex reads, 96 B FP64 box + 1 B
 #            active written, 32 B of node slot written, 64 B per internal node read.
-def algorithmic_bytes(c, n):
+def algorithmic_bytes(c, n, fused=False):
     walk = n * (96 + 4 + 1) + (n - 1) * 64 + c["leaf_pairs"] * (96 + 4 + 8)
+    refit = n * (12 + 144 + 96 + 1 + 32) + (n - 1) * 64
+    if fused:
+        narrow = c["leaf_pairs"] * (8 + 26 + 144) + 8 * c["discrete"] + (c["vf"] + c["ee"]) * 192 + 25 * c["hits"]
+        return {"walk": walk, "expand": 0, "narrow": narrow, "refit": refit}
     expand = c["leaf_pairs"] * (8 + 26 + 144) + 16 * (c["vf"] + c["ee"]) + 8 * c["discrete"]
     narrow = (c["vf"] + c["ee"]) * (16 + 192) + 25 * c["hits"]
-    refit = n * (12 + 144 + 96 + 1 + 32) + (n - 1) * 64
     return {"walk": walk, "expand": expand, "narrow": narrow, "refit": refit}
 
 
 def per_unit_figures():
-    """The per-unit figures of the committed ncu summary
-    (profiles/dram_traffic_per_unit.txt): DRAM bytes per unit of each stage
-    and FP64 flops per VF / EE stencil of the narrow phase."""
+    """The committed per-unit figures: DRAM bytes per unit of each stage from
+    the ncu summary (profiles/dram_traffic_per_unit.txt) and FP64 flops per
+    VF / EE stencil of the narrow phase counted on the oracle
+    (profiles/narrow_flops_per_stencil.txt, oracle/count_flops.py)."""
     per = {}
-    try:
-        with open(os.path.join(ROOT, "profiles", "dram_traffic_per_unit.txt")) as f:
-            for line in f:
-                parts = line.split()
-                if len(parts) == 2 and not line.startswith("#"):
-                    per[parts[0]] = float(parts[1])
-    except OSError:
-        return {}
+    for name in ("dram_traffic_per_unit.txt", "narrow_flops_per_stencil.txt"):
+        try:
+            with open(os.path.join(ROOT, "profiles", name)) as f:
+                for line in f:
+                    parts = line.split()
+                    if len(parts) == 2 and not line.startswith("#"):
+                        per[parts[0]] = float(parts[1])
+        except OSError:
+            pass
     return per
 
 
@@ -165,19 +174,23 @@ FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
 def fp64_roofline(c, narrow_ms, per=None):
-    """FP64 roofline of the narrow phase: the captured flops per VF and EE
-    stencil times this run's stencils, over the narrow stage's time."""
+    """FP64 roofline of the narrow phase: the flops per VF and EE stencil
+    counted on the oracle (the necessary work: add, multiply, divide and
+    square root one flop each) times this run's stencils, over the narrow
+    stage's time."""
     per = per_unit_figures() if per is None else per
-    if "narrow_fp64_flops_per_vf" not in per or not narrow_ms or narrow_ms <= 0:
+    if "narrow_flops_per_vf" not in per or not narrow_ms or narrow_ms <= 0:
         return None
-    flops = per["narrow_fp64_flops_per_vf"] * c["vf"] + per.get("narrow_fp64_flops_per_ee", 0.0) * c["ee"]
+    flops = per["narrow_flops_per_vf"] * c["vf"] + per.get("narrow_flops_per_ee", 0.0) * c["ee"]
     achieved = flops / (narrow_ms / 1e3) / 1e12
     return {"achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS,
-            "flops": flops, "peak_source": "nominal: 148 SMs x 64 FP64 FMA lanes x 2 flops x 1965 MHz",
-            "flops_source": "ncu thread-level DADD + DMUL + 2 DFMA per stencil, per kind"}
+            "flops": flops, "peak_source": "nominal: 148 SMs x 64 FP64 FMA lanes x 2 flops x 1965 MHz "
+                                           "(no measured FP64 peak exists for this pool)",
+            "flops_source": "oracle/count_flops.py: necessary FP64 operations per stencil, per kind "
+                            "(profiles/narrow_flops_per_stencil.txt)"}
 
 
-def measured_traffic(c):
+def measured_traffic(c, fused=False):
     """DRAM bytes per stage of one step from the per-unit figures of the
     committed ncu summary, scaled by this run's unit counts."""
     per = per_unit_figures()
@@ -187,6 +200,10 @@ def measured_traffic(c):
     sten = c["vf"] + c["ee"]
     if "walk_bytes_per_leaf_pair" in per:
         out["walk"] = per["walk_bytes_per_leaf_pair"] * c["leaf_pairs"]
+    if fused:
+        if "fused_bytes_per_stencil" in per:
+            out["narrow"] = per["fused_bytes_per_stencil"] * sten
+        return out
     if "expand_bytes_per_stencil" in per:
         out["expand"] = per["expand_bytes_per_stencil"] * sten
     if "narrow_bytes_per_stencil" in per:
@@ -218,44 +235,47 @@ def aggregate(dist, device, total_s, work):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own CPU implementation (the oracle
+    build of the unmodified reference sources, all host threads) on the same
+    workload and step as the device arm -- the 1025 x 1025 wavy cloth, one
+    first update (full build) untimed, then per step update(V0, V1, F) with
+    V1 alternating between the two seeded draws (the reference rebuilds its
+    Kd-tree on every update) and traverse with the default ACCD; hooks are
+    no-op counters.  K steps are timed after W; rank 0 only."""
     if rank != 0:
         return 0
     from mclccd_b200 import scenes
     from oracle.ref import REF_SO, Port, Reference
-    rows = 257
-    V0, V1a, F, eta = scenes.wavy_cloth(args.n, seed=0, rows=rows)
+    V0, V1a, F, eta = scenes.wavy_cloth(args.n, seed=0)
     V1b = scenes.wavy_redraw(V0, 1)
     if os.path.exists(REF_SO):
         R, kind = Reference(), "reference"
-        rec = R.run(V0, V1b, F, eta)
-        n_sten = len(rec["cand_sten"])
         cores = R.L.ref_threads()
-    else:
-        R, kind = None, "port"
-        p = Port().run(V0, V1b, F, eta)
-        n_sten = len(p["cand_sten"])
-        cores = 1
-    times = []
-    for it in range(args.warmup + args.steps):
-        if R is not None:
-            r = R.time(V0, V1a, F, eta, V1b=V1b)
-            ms = r["ms_update_again"] + r["ms_traverse"]
-        else:
+        r = R.time_steps(V0, V1a, V1b, F, eta, args.warmup + args.steps)
+        ms_all, sten_all = r["ms"], r["stencils"]
+    else:   # the oracle restatement, single-threaded, one step at a time
+        R, kind, cores = None, "port", 1
+        ms_all, sten_all = [], []
+        for it in range(args.warmup + args.steps):
+            V1 = V1b if it % 2 == 0 else V1a
             t0 = time.perf_counter()
-            Port().run(V0, V1b, F, eta)
-            ms = (time.perf_counter() - t0) * 1e3
-        if it >= args.warmup:
-            times.append(ms)
+            p = Port().run(V0, V1, F, eta)
+            ms_all.append((time.perf_counter() - t0) * 1e3)
+            sten_all.append(len(p["cand_sten"]))
+    times = ms_all[args.warmup:]
+    sten = sten_all[args.warmup:]
     ms = float(np.mean(times))
-    val = n_sten / (ms / 1e3)
-    sample = (f"{rows}-row strip of the {args.n}x{args.n} wavy cloth ({len(F)} tris, {n_sten} stencils): "
-              f"update + traverse per step")
+    val = float(np.sum(sten)) / (np.sum(times) / 1e3)
+    sample = (f"the full workload, {args.steps} timed steps after {args.warmup}: second update (same F, V1 "
+              f"alternating two draws) + traverse with the default ACCD, {len(F)} tris, "
+              f"{int(np.mean(sten))} stencils per step")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"wavy cloth {args.n}x{args.n} (2,097,152 tris), thickness 1e-4; "
-                                   f"reference steps on a {rows}-row strip", "tris_per_step": int(len(F)),
-                       "stencils_per_step": int(n_sten)},
+            "config": {"workload": f"wavy cloth {args.n}x{args.n} ({len(F)} tris), thickness 1e-4, refit-only "
+                                   "update + traverse + ACCD per step (F unchanged, V1 alternates two seeded draws)",
+                       "tris": int(len(F)), "stencils_per_step": int(np.mean(sten)),
+                       "step_ms_all": [float(x) for x in times]},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -355,22 +375,33 @@ def run_b200(args, rank, world, local):
     pstats = tree.precision_stats()
     stage = {k: float(np.median([s[k] for s in stages])) for k in stages[0]}
 
-    # roofline of the dominant kernel: algorithmic bytes / its device time
-    ab = algorithmic_bytes(c, n)
+    # roofline of the dominant kernel.  The narrow phase is bound by the FP64
+    # pipe: flops counted on the oracle / its device time against the FP64
+    # peak; the other stages by memory: algorithmic bytes / time.
+    tuning = tree.get_tuning()
+    fused = prec == PREC_FP64 and tuning["narrow_fused"] == 1 and tuning["accd_rebin"] == 0
+    ab = algorithmic_bytes(c, n, fused)
     kt = {"walk": stage["walk"], "expand": stage["expand"], "narrow": stage["narrow"], "refit": stage["refit"]}
     top = max(kt, key=kt.get)
     peak, src = measured_peaks()
-    achieved = ab[top] / (kt[top] / 1e3) / 1e9
-    tr = measured_traffic(c)
-    roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": tr.get(top), "peak_source": src,
-            "traffic_source": "ncu dram bytes per unit (profiles/dram_traffic_per_unit.txt) x this run's units",
-            "algorithmic_bytes": ab[top], "kernel_ms": kt[top],
-            "note": "narrow = the VF and EE ACCD launches of one step; they are FP64-pipe bound "
-                    "(49-54% of peak in the committed ncu summary of these kernels), their vertex gathers hit L2",
-            "all": {k: {"ms": kt[k], "GB/s": ab[k] / (kt[k] / 1e3) / 1e9 if kt[k] > 0 else None,
-                        "traffic": tr.get(k)} for k in kt},
-            "narrow_fp64": fp64_roofline(c, kt["narrow"])}
+    tr = measured_traffic(c, fused)
+    fp = fp64_roofline(c, kt["narrow"])
+    hbm = {k: {"ms": kt[k], "algorithmic_bytes": ab[k],
+               "GB/s": ab[k] / (kt[k] / 1e3) / 1e9 if kt[k] > 0 else None,
+               "frac": ab[k] / (kt[k] / 1e3) / 1e9 / peak if kt[k] > 0 else None,
+               "traffic": tr.get(k)} for k in kt}
+    if top == "narrow" and fp is not None:
+        roof = {"bound": "fp64", "kernel": top, "achieved": fp["achieved"], "peak": fp["peak"], "unit": "TFLOP/s",
+                "frac": fp["frac"], "traffic": tr.get(top), "peak_source": fp["peak_source"], "flops": fp["flops"],
+                "flops_source": fp["flops_source"], "kernel_ms": kt[top]}
+    else:
+        roof = {"bound": "hbm", "kernel": top, "achieved": hbm[top]["GB/s"], "peak": peak, "unit": "GB/s",
+                "frac": hbm[top]["frac"], "traffic": tr.get(top), "peak_source": src,
+                "algorithmic_bytes": ab[top], "kernel_ms": kt[top]}
+    roof.update({
+        "narrow_form": "fused (expansion + discrete test + ACCD in one kernel)" if fused else "stencil lists",
+        "traffic_source": "ncu dram bytes per unit (profiles/dram_traffic_per_unit.txt) x this run's units",
+        "hbm_peak_gbs": peak, "hbm_peak_source": src, "stages_hbm": hbm, "narrow_fp64": fp})
 
     # end to end through the C ABI from pinned host memory
     e2e = None

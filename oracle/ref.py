@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libmclccd_ref.so")
 PORT_SO = os.path.join(HERE, "_build", "liboracle_port.so")
+FLOPS_SO = os.path.join(HERE, "_build", "liboracle_flops.so")
 
 F_REPTRI, F_THREADED, F_DISCRETE, F_CONTINUOUS, F_RECORD_CAND, F_ONE_SIDED, F_FLOAT = 1, 2, 4, 8, 16, 32, 64
 DEFAULT_FLAGS = F_REPTRI | F_THREADED | F_DISCRETE | F_CONTINUOUS
@@ -84,6 +85,8 @@ class Reference:
                                _dp, _dp, _dp, C.POINTER(C.c_longlong)]
         L.ref_time.restype = C.c_longlong
         L.ref_threads.restype = C.c_int
+        L.ref_time_steps.argtypes = [C.c_int, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_double, C.c_int, _dp,
+                                     C.POINTER(C.c_longlong)]
         self.L = L
 
     def run(self, V0, V1, F, box_eta, vf_eta=None, ee_eta=None, flags=DEFAULT_FLAGS | F_RECORD_CAND, active=None):
@@ -162,6 +165,19 @@ class Reference:
                              C.byref(a), C.byref(b), C.byref(c), C.byref(nd))
         return dict(ms_update_first=a.value, ms_update_again=b.value, ms_traverse=c.value,
                     n_hits=nh, n_discrete=nd.value, threads=self.L.ref_threads())
+
+
+    def time_steps(self, V0, V1a, V1b, F, eta, steps):
+        """The benchmark step on the reference (ref_time_steps): per step the
+        update + traverse ms and the candidate stencils, V1 alternating
+        between V1b and V1a after an untimed first update with V1a."""
+        V0, V1a, V1b = (np.ascontiguousarray(x, np.float64) for x in (V0, V1a, V1b))
+        F = np.ascontiguousarray(F, np.int32)
+        ms = np.zeros(steps); st = np.zeros(steps, np.int64)
+        self.L.ref_time_steps(V0.shape[1], _p(V0, C.c_double), _p(V1a, C.c_double), _p(V1b, C.c_double),
+                              _p(F, C.c_int), F.shape[0], F.shape[1], eta, steps, _p(ms, C.c_double),
+                              st.ctypes.data_as(C.POINTER(C.c_longlong)))
+        return {"ms": [float(x) for x in ms], "stencils": [int(x) for x in st], "threads": self.L.ref_threads()}
 
 
 FLAG_ACTIVE = 1 << 6
@@ -301,3 +317,34 @@ class Port:
         st = self.L.adj_ref_fd(dim, int(is_vf), _p(v0, C.c_double), _p(v1, C.c_double), eta, toi, h,
                                _p(out, C.c_double))
         return st, out
+
+
+class Flops:
+    """FP64 flop count of the narrow phase on the oracle (oracle/flops.cpp):
+    per kind, the reference loop's flops and the necessary flops (the
+    device's form), with both forms' (hit, toi) for checking."""
+
+    def __init__(self, path: str = FLOPS_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"flop counter not built: {path} (make -C oracle port)")
+        L = C.CDLL(path)
+        L.flops_accd.argtypes = [C.c_int, _dp, _dp, _ip, _ucp, C.c_longlong, C.c_double, C.c_double,
+                                 C.POINTER(C.c_longlong), _ip, _dp, _ip, _dp]
+        self.L = L
+
+    def accd(self, V0, V1, sten, is_vf, vf_eta, ee_eta=None):
+        V0 = np.ascontiguousarray(V0, np.float64); V1 = np.ascontiguousarray(V1, np.float64)
+        s = np.ascontiguousarray(sten, np.int32).reshape(-1, 4)
+        v = np.ascontiguousarray(is_vf, np.uint8).reshape(-1)
+        n = len(s)
+        out = np.zeros(8, np.int64)
+        hit = np.empty(n, np.int32); toi = np.empty(n); hf = np.empty(n, np.int32); tf = np.empty(n)
+        self.L.flops_accd(V0.shape[1], _p(V0, C.c_double), _p(V1, C.c_double), _p(s, C.c_int), _p(v, C.c_ubyte), n,
+                          vf_eta, vf_eta if ee_eta is None else ee_eta, out.ctypes.data_as(C.POINTER(C.c_longlong)),
+                          _p(hit, C.c_int), _p(toi, C.c_double), _p(hf, C.c_int), _p(tf, C.c_double))
+        kinds = {}
+        for name, k in (("ee", 0), ("vf", 1)):
+            o = out[4 * k: 4 * k + 4]
+            kinds[name] = {"stencils": int(o[0]), "reference_flops": int(o[1]), "necessary_flops": int(o[2]),
+                           "reference_distances": int(o[3])}
+        return kinds, (hit, toi), (hf, tf)

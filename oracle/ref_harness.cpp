@@ -301,6 +301,45 @@ long long ref_time(int dim, const double *V0, const double *V1, const double *V1
     return nh.load();
 }
 
+// The benchmark step on the reference, repeated: one untimed first update
+// (V1a), then per step i update(V0, V1[i % 2], P) with V1[0] = V1b, V1[1] =
+// V1a, and traverse; hooks are no-op counters (filter_pair and narrow_phase
+// unset, as in the reference's defaults).  ms[i] = update + traverse of step
+// i.  stencils[i] = the candidate stencils of that step, counted in an extra
+// untimed traverse per draw with a counting filter_pair.
+void ref_time_steps(int dim, const double *V0, const double *V1a, const double *V1b, const int *P, int np, int pdim,
+                    double eta, int steps, double *ms, long long *stencils)
+{
+    using clk = std::chrono::steady_clock;
+    std::atomic<long long> nh(0), nd(0), nc(0);
+    auto go = [&](auto &tree) {
+        tree.options.box_eta = eta; tree.options.vf_ccd_eta = eta; tree.options.ee_ccd_eta = eta;
+        tree.append_pair = [&](const Eigen::Vector4i &, bool, const double &) { nh.fetch_add(1, std::memory_order_relaxed); };
+        tree.append_discrete = [&](int, int) -> bool { nd.fetch_add(1, std::memory_order_relaxed); return false; };
+        const double *V1s[2] = {V1b, V1a};
+        long long per_draw[2] = {-1, -1};
+        tree.update(V0, V1a, P, np, pdim);
+        for (int i = 0; i < steps; ++i) {
+            const double *V1 = V1s[i % 2];
+            auto t0 = clk::now();
+            tree.update(V0, V1, P, np, pdim);
+            tree.traverse(V0, V1, P);
+            auto t1 = clk::now();
+            ms[i] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+            if (per_draw[i % 2] < 0) {
+                nc = 0;
+                tree.filter_pair = [&](const Eigen::Vector4i &, bool) -> bool { nc.fetch_add(1, std::memory_order_relaxed); return false; };
+                tree.traverse(V0, V1, P);
+                tree.filter_pair = nullptr;
+                per_draw[i % 2] = nc.load();
+            }
+            stencils[i] = per_draw[i % 2];
+        }
+    };
+    if (dim == 3) { mcl::BVHTree<double, 3> t; go(t); }
+    else { mcl::BVHTree<double, 2> t; go(t); }
+}
+
 int ref_threads() { return tbb::compat_thread_count(); }
 
 } // extern "C"

@@ -49,15 +49,39 @@ def test_single_rank_aggregate_is_local():
 
 
 def test_fp64_roofline_of_the_narrow_phase():
-    # flops per stencil from the committed ncu summary x stencils / time,
-    # against 148 SMs x 64 FP64 lanes x 2 flops x 1965 MHz
+    # flops per stencil counted on the oracle (profiles/narrow_flops_per_stencil.txt)
+    # x stencils / time, against 148 SMs x 64 FP64 lanes x 2 flops x 1965 MHz
     import bench
     per = bench.per_unit_figures()
-    assert per["narrow_fp64_flops_per_vf"] > 0 and per["narrow_fp64_flops_per_ee"] > 0
+    assert per["narrow_flops_per_vf"] > 0 and per["narrow_flops_per_ee"] > 0
     assert per["walk_bytes_per_leaf_pair"] > 0
     c = {"vf": 1_000_000, "ee": 2_000_000}
     r = bench.fp64_roofline(c, 1.0, per)
-    want = (per["narrow_fp64_flops_per_vf"] * 1e6 + per["narrow_fp64_flops_per_ee"] * 2e6) / 1e-3 / 1e12
+    want = (per["narrow_flops_per_vf"] * 1e6 + per["narrow_flops_per_ee"] * 2e6) / 1e-3 / 1e12
     assert abs(r["achieved"] - want) < 1e-9 and r["unit"] == "TFLOP/s"
     assert abs(r["peak"] - 37.22) < 0.01 and abs(r["frac"] - want / r["peak"]) < 1e-12
     assert bench.fp64_roofline(c, 0.0, per) is None and bench.fp64_roofline(c, 1.0, {}) is None
+
+
+def test_committed_flops_match_the_oracle_count():
+    # the frozen figures are what oracle/count_flops.py reports for the strip
+    # of the benchmark cloth (checked on a smaller strip of the same cloth,
+    # whose per-stencil counts agree within a few percent)
+    import bench
+    from mclccd_b200 import scenes
+    from oracle.count_flops import count
+    per = bench.per_unit_figures()
+    kinds, _ = count(*scenes.wavy_cloth(1025, seed=0, rows=65))
+    for k in ("vf", "ee"):
+        got = kinds[k]["necessary_flops"] / kinds[k]["stencils"]
+        assert abs(got - per[f"narrow_flops_per_{k}"]) < 0.05 * per[f"narrow_flops_per_{k}"], (k, got)
+
+
+def test_algorithmic_bytes_forms():
+    import bench
+    c = {"leaf_pairs": 10, "vf": 20, "ee": 30, "discrete": 2, "hits": 25}
+    lists = bench.algorithmic_bytes(c, 100)
+    fused = bench.algorithmic_bytes(c, 100, fused=True)
+    assert fused["expand"] == 0 and fused["walk"] == lists["walk"] and fused["refit"] == lists["refit"]
+    # the fused form neither writes nor reads the 16 B stencil records
+    assert fused["narrow"] == lists["expand"] + lists["narrow"] - 2 * 16 * (c["vf"] + c["ee"])
