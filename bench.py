@@ -438,6 +438,10 @@ def run_b200(args, rank, world, local):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e_total * 1e3 / args.steps}
 
+    dropin = None
+    if rank == 0 and world == 1 and not args.no_e2e:
+        dropin = measure_dropin(args, V0, V1a, V1b, F, eta, c)
+
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         forms = measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev)
@@ -467,12 +471,49 @@ def run_b200(args, rank, world, local):
             "gpu_launches": int(launches), "roofline": roof, "clocks": clk}
     if e2e is not None:
         line["e2e"] = e2e
+    if dropin is not None:
+        line["e2e_dropin"] = dropin
     if forms is not None:
         line["forms"] = forms
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
+
+
+def measure_dropin(args, V0, V1a, V1b, F, eta, c):
+    """End to end through the C++ drop-in (tests/cpp/dropin_bench.cpp):
+    mcl::BVHTree<double, 3> with append_pair / append_discrete set, the
+    reference's update(V0, V1, F, nf, 3) + traverse(V0, V1, F) on host arrays
+    per step, hooks called for every hit; wall time per step."""
+    exe_dir = tempfile.mkdtemp(prefix="mclccd_dropin_")
+    try:
+        exe = os.path.join(exe_dir, "dropin_bench")
+        subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "dropin_bench.cpp"), "-L", os.path.join(ROOT, "mclccd_b200"),
+                        "-lmclccd_b200", "-Wl,-rpath," + os.path.join(ROOT, "mclccd_b200"), "-o", exe], check=True)
+        scene = os.path.join(exe_dir, "scene.bin")
+        with open(scene, "wb") as f:
+            f.write(np.array([len(V0), len(F)], np.int32).tobytes())
+            f.write(np.array([eta], np.float64).tobytes())
+            for a in (V0, V1a, V1b):
+                f.write(np.ascontiguousarray(a, np.float64).tobytes())
+            f.write(np.ascontiguousarray(F, np.int32).tobytes())
+        out = subprocess.run([exe, scene, str(args.warmup), str(args.steps)], check=True, capture_output=True,
+                             text=True).stdout
+        r = json.loads(out.strip().splitlines()[-1])
+    except Exception as e:   # reported, never fatal to the headline line
+        return {"error": f"{type(e).__name__}: {e}"}
+    finally:
+        shutil.rmtree(exe_dir, ignore_errors=True)
+    ms = float(np.mean(r["ms"]))
+    sten = c["vf"] + c["ee"]
+    return {"value": sten / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "step_ms_all": r["ms"],
+            "h2d_bytes_per_step": int(V0.nbytes + V1a.nbytes + F.nbytes),
+            "d2h_bytes_per_step": int(r["hits"] * (16 + 1 + 8) + r["discrete"] * 8),
+            "hits_delivered": r["hits"], "discrete_delivered": r["discrete"],
+            "api": "C++ mcl::BVHTree<double,3>: update(V0,V1,F,nf,3) + traverse(V0,V1,F) on host arrays, "
+                   "append_pair / append_discrete called for every result (wall clock)"}
 
 
 def measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev):

@@ -24,6 +24,8 @@
 #ifndef MCLCCD_B200_H
 #define MCLCCD_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -70,6 +72,10 @@ int mclccd_create(int dim, mclccd_tree **out);
 /* Replaces: ~BVHTree().  Frees every device buffer the handle owns. */
 int mclccd_destroy(mclccd_tree *tree);
 
+/* Sizes of the last update: vertex count (the derived one when the update
+ * passed nv = 0), primitive count and primitive width (any may be NULL). */
+int mclccd_tree_size(const mclccd_tree *tree, int *nv, int *np, int *pdim);
+
 /* Replaces: writes to BVHTree::options (BVHTree.hpp:42-64). */
 int mclccd_set_options(mclccd_tree *tree, double box_eta, double vf_ccd_eta, double ee_ccd_eta, unsigned flags);
 /* Reads them back (update() clamps the two gaps to box_eta, BVHTree.cpp:39-40). */
@@ -86,9 +92,11 @@ int mclccd_set_precision(mclccd_tree *tree, int precision);
 
 /* Replaces: BVHTree::update(const T*V0, const T*V1, const int*P, int np,
  * int pdim, const int*active) (BVHTree.hpp:81-82, BVHTree.cpp:27-126).
- * nv is new: the device needs the vertex count to copy/validate V0, V1.
- * active is an optional per-vertex int mask (NULL = all active).  When np,
- * pdim, nv and the bytes of P equal the previous update, only the boxes are
+ * nv is new: the device needs the vertex count to copy/validate V0, V1;
+ * nv = 0 takes it as 1 + the largest index in P, as the reference's
+ * signature implies (found on the device, no host pass over P).  active is
+ * an optional per-vertex int mask (NULL = all active).  When np, pdim, nv
+ * and the bytes of P equal the previous update, only the boxes are
  * refitted; otherwise the hierarchy is rebuilt.  np == 0 clears the tree. */
 int mclccd_update(mclccd_tree *tree, const double *V0, const double *V1, int nv, const int *P, int np, int pdim,
                   const int *active, int mem_kind);
@@ -181,8 +189,10 @@ int mclccd_precision_stats(const mclccd_tree *tree, long long *n_fp64, long long
  * calls return MCLCCD_ERR_SCRATCH_LIMIT (device-memory calls use only the
  * status word and have no size limit).  The first call on each device looks
  * up the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race on it. */
+ * before any stream capture.  The address is kept for the life of the
+ * process, so do not call this entry point after cudaDeviceReset (or any
+ * reset of the device's primary context) in the same process.  All calls
+ * share the array: calls that overlap on the GPU race on it. */
 #define MCLCCD_STATIC_SCRATCH_BYTES (32u << 20)
 int mclccd_narrow_phase_bulk_static(int dim, const double *V0, const double *V1, int nv, const int *sten,
                                     const unsigned char *is_vf, long long n, double vf_ccd_eta, double ee_ccd_eta,
@@ -298,6 +308,23 @@ typedef struct {
 } mclccd_tree_view;
 int mclccd_get_tree_view(const mclccd_tree *tree, mclccd_tree_view *view);
 
+/* Replaces: the host side of BVHTree::traverse(BVHTraverse<T,DIM>*)
+ * (BVHTree.hpp:17-27, 96; BVHTree.cpp:162-166), which walks the tree on the
+ * host calling a visitor's virtual intersectVolume / intersectObject: copies
+ * the tree of the last update into caller host arrays (any may be NULL):
+ * nodes (n_leaves - 1 records of 128 B, layout as in mclccd_tree_view),
+ * leaf_box (n_leaves x 4 x dim doubles), leaf_prim (n_leaves ints) and
+ * leaf_flags (n_leaves bytes: bits 0-2 vertex slots and 3-5 edge slots
+ * represented, bit 6 active), all in sorted leaf order.  The C++ drop-in
+ * (include/mclccd_b200/BVHTree.hpp) uses it for its visitor overload. */
+int mclccd_get_tree_host(mclccd_tree *tree, void *nodes, double *leaf_box, int *leaf_prim, unsigned char *leaf_flags);
+
+/* No counterpart in the reference: page-locked host memory from the CUDA
+ * runtime, for callers that stage results without including CUDA headers
+ * (device-to-host copies into it run asynchronously at full PCIe speed). */
+int mclccd_host_alloc(size_t bytes, void **ptr);
+int mclccd_host_free(void *ptr);
+
 /* Input forms other than row-major double (no counterpart in the
  * reference; its Eigen overloads copy to RowMajor, BVHTree.hpp:151-186).
  * One device pass converts them into the arrays the path runs on, so the
@@ -346,12 +373,16 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
  * walk only), and overlap (K = 2..16: the queries in K chunks, the walk of
  * chunk c + 1 running while chunk c is expanded and scored, on two internal
  * streams; 0: in sequence; FP64 and one-sided forms only), the FP64 narrow
- * phase form (1, the default: one kernel takes the leaf pairs to stencils,
- * runs the discrete test and ACCD on them in per-warp batches of one kind,
- * and counts the candidate lists without writing them (mclccd_get_candidates
- * rebuilds them on request); 0: the expansion kernel writes the VF and EE
- * lists and one ACCD kernel runs over each) and the grid size (in blocks) of
- * that fused kernel.  Results do not depend on any of them. */
+ * phase form (0, the default: the expansion kernel writes the VF and EE
+ * lists and one ACCD kernel runs over each; 1: one kernel takes the leaf
+ * pairs to stencils, runs the discrete test and ACCD on them in per-warp
+ * batches of one kind, and counts the candidate lists without writing them
+ * (mclccd_get_candidates rebuilds them on request) -- measured slower), the grid size (in blocks) of
+ * that fused kernel, and the refill walk (1: persistent warps take chunks of
+ * 32 queries, run their window part, and refill lanes whose tree walk is
+ * done from a per-warp pool of queries, so lanes do not idle behind the
+ * longest walk of their warp; window 8, 16 or 32; 0: one query per thread
+ * start to end).  Results do not depend on any of them. */
 #define MCLCCD_TUNE_EXPAND_GRID 0
 #define MCLCCD_TUNE_ACCD_GRID 1
 #define MCLCCD_TUNE_WALK_PACKET 2
@@ -360,7 +391,8 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
 #define MCLCCD_TUNE_OVERLAP 5
 #define MCLCCD_TUNE_NARROW_FUSED 6
 #define MCLCCD_TUNE_FUSED_GRID 7
-#define MCLCCD_TUNE_COUNT 8
+#define MCLCCD_TUNE_WALK_REFILL 8
+#define MCLCCD_TUNE_COUNT 9
 int mclccd_set_tuning(mclccd_tree *tree, int key, int value);
 int mclccd_get_tuning(const mclccd_tree *tree, int key, int *value);
 

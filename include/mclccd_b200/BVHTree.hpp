@@ -16,6 +16,16 @@
 //     only filter_pair is set).
 // EE stencils and discrete pairs come with the lower primitive index first.
 // Errors throw mcl::CCDError (the reference asserts or silently returns).
+//
+// traverse(BVHTraverse<T, DIM>*) runs a visitor over a host copy of the
+// tree, with the reference's types (BVHTraverse, BVHLeaf, BoundingBox) and
+// Eigen's BVIntersect order: a node's child volumes are offered to
+// intersectVolume, then its leaves to intersectObject (true stops).
+// Volumes are the FP32 node boxes rounded outward (never smaller than the
+// reference's merged boxes); leaves carry their exact FP64 boxes.
+//
+// traverse(V0, V1, P) given the very arrays (the same pointers) of the last
+// update reuses their device copies instead of copying them again.
 #pragma once
 
 #include "../mclccd_b200.h"
@@ -45,6 +55,85 @@ typedef Eigen::Vector4i Stencil;
 #else
 typedef std::array<int, 4> Stencil;
 #endif
+
+#ifdef MCLCCD_B200_HAVE_EIGEN
+template <typename T, int DIM>
+using AlignedBoxT = Eigen::AlignedBox<T, DIM>;
+typedef Eigen::Vector3i RepFlags;
+inline RepFlags rep_all() { return RepFlags(1, 1, 1); }
+#else
+// Without Eigen: the part of Eigen::AlignedBox<T, DIM> a visitor uses.
+template <typename T, int DIM>
+class AlignedBoxT {
+public:
+    typedef std::array<T, DIM> VectorType;
+    AlignedBoxT() { setEmpty(); }
+    VectorType &min() { return lo_; }
+    VectorType &max() { return hi_; }
+    const VectorType &min() const { return lo_; }
+    const VectorType &max() const { return hi_; }
+    void setEmpty()
+    {
+        lo_.fill(std::numeric_limits<T>::max());
+        hi_.fill(std::numeric_limits<T>::lowest());
+    }
+    bool isEmpty() const
+    {
+        for (int k = 0; k < DIM; ++k)
+            if (hi_[k] < lo_[k]) return true;
+        return false;
+    }
+    bool contains(const VectorType &p) const
+    {
+        for (int k = 0; k < DIM; ++k)
+            if (p[k] < lo_[k] || hi_[k] < p[k]) return false;
+        return true;
+    }
+    bool intersects(const AlignedBoxT &b) const
+    {
+        for (int k = 0; k < DIM; ++k)
+            if (hi_[k] < b.lo_[k] || b.hi_[k] < lo_[k]) return false;
+        return true;
+    }
+
+private:
+    VectorType lo_, hi_;
+};
+typedef std::array<int, 3> RepFlags;
+inline RepFlags rep_all() { return RepFlags{{1, 1, 1}}; }
+#endif
+
+// BVHLeaf.hpp:12-28: the swept box, with the t = 0 and t = 1 boxes and the
+// active flag.
+template <typename T, int DIM>
+class BoundingBox : public AlignedBoxT<T, DIM> {
+public:
+    bool active = true;
+    AlignedBoxT<T, DIM> t0, t1;
+    virtual ~BoundingBox() {}
+};
+
+// BVHLeaf.hpp:30-52: primitive index, representative vertex / edge flags, box.
+template <typename T, int DIM>
+class BVHLeaf {
+public:
+    typedef BoundingBox<T, DIM> BoxType;
+    int idx = -1;
+    RepFlags v = rep_all(), e = rep_all();
+    BoxType box;
+    virtual ~BVHLeaf() {}
+};
+
+// BVHTree.hpp:17-27: visitor of traverse(BVHTraverse *).
+template <typename T, int DIM>
+class BVHTraverse {
+public:
+    typedef BVHLeaf<T, DIM> ObjectType;
+    typedef typename BVHLeaf<T, DIM>::BoxType VolumeType;
+    virtual ~BVHTraverse() {}
+    virtual bool intersectVolume(const VolumeType &) = 0;   // true: descend into this volume
+    virtual bool intersectObject(const ObjectType &) = 0;   // true: stop the traversal
+};
 
 class CCDError : public std::runtime_error {
 public:
@@ -83,12 +172,17 @@ public:
     BVHTree &operator=(const BVHTree &) = delete;
 
     // Reference signature (BVHTree.hpp:81-82).  It carries no vertex count, so
-    // the count is taken as 1 + the largest index in P.
+    // the count is taken as 1 + the largest index in P, found on the device
+    // (float trees, whose coordinates are staged first, scan P here).
     void update(const T *V0, const T *V1, const int *P, int np, int pdim, const int *active = nullptr)
     {
         int nv = 0;
-        for (long long i = 0; i < (long long)np * pdim; ++i) nv = std::max(nv, P[i] + 1);
+        if constexpr (kFloat)
+            for (long long i = 0; i < (long long)np * pdim; ++i) nv = std::max(nv, P[i] + 1);
         update(V0, V1, nv, P, np, pdim, active, MCLCCD_MEM_HOST);
+        upd_V0_ = V0;
+        upd_V1_ = V1;
+        upd_P_ = P;
     }
 
     // With an explicit vertex count; mem_kind MCLCCD_MEM_DEVICE takes device
@@ -102,15 +196,25 @@ public:
         else rc = mclccd_update(h_, V0, V1, nv, P, np, pdim, active, mem_kind);
         pull_options();
         check(rc);
+        if (nv == 0) check(mclccd_tree_size(h_, &nv, nullptr, nullptr));
         nv_ = nv;
         np_ = np;
         mem_ = mem_kind;
+        upd_V0_ = upd_V1_ = nullptr;
+        upd_P_ = nullptr;
+        ++rev_;
     }
 
     // Reference signature (BVHTree.hpp:86).  Runs the device pipeline on the
     // given arrays (same side as the last update), then calls the hooks.
     void traverse(const T *V0, const T *V1, const int *P) const
     {
+        // the arrays of the last update: their device copies are current
+        if (V0 && V0 == upd_V0_ && V1 == upd_V1_ && P == upd_P_ && mem_ == MCLCCD_MEM_HOST &&
+            !(filter_pair && !narrow_phase)) {
+            traverse();
+            return;
+        }
         auto *self = const_cast<BVHTree *>(this);
         self->push_options();
         if constexpr (!kFloat) {
@@ -132,6 +236,31 @@ public:
         if constexpr (kFloat) check(mclccd_traverse_f32(h_, nullptr, nullptr, 0, nullptr, mem_));
         else check(mclccd_traverse(h_, nullptr, nullptr, 0, nullptr, mem_));
         self->dispatch(nullptr, nullptr);
+    }
+
+    // Reference signature (BVHTree.hpp:96, BVHTree.cpp:162-166): the visitor
+    // over a host copy of the tree (fetched once per update).
+    void traverse(BVHTraverse<T, DIM> *traverser) const
+    {
+        if (!traverser || np_ < 1) return;
+        auto *self = const_cast<BVHTree *>(this);
+        self->fetch_tree();
+        if (np_ == 1) {
+            traverser->intersectObject(self->leaf_object(0));
+            return;
+        }
+        std::vector<int> pending(1, 0);
+        while (!pending.empty()) {
+            const int node = pending.back();
+            pending.pop_back();
+            const HostNode &nd = tree_nodes_[node];
+            const int split = nd.d[0], meta = nd.d[1];
+            for (int side = 0; side < 2; ++side)
+                if (!(meta & (1 << side)) && traverser->intersectVolume(node_volume(nd, side)))
+                    pending.push_back(split + side);
+            for (int side = 0; side < 2; ++side)
+                if ((meta & (1 << side)) && traverser->intersectObject(self->leaf_object(split + side))) return;
+        }
     }
 
 #ifdef MCLCCD_B200_HAVE_EIGEN
@@ -241,11 +370,95 @@ private:
 #endif
     mclccd_tree *h_ = nullptr;
     int nv_ = 0, np_ = 0, mem_ = MCLCCD_MEM_HOST;
-    // hit staging for streamed(), kept across calls (capacity from the last count)
-    std::unique_ptr<int[]> out_s_;
-    std::unique_ptr<unsigned char[]> out_v_;
-    std::unique_ptr<double[]> out_t_;
+    const T *upd_V0_ = nullptr, *upd_V1_ = nullptr;   // host arrays of the last update (reference signature)
+    const int *upd_P_ = nullptr;
+    long long rev_ = 0, tree_rev_ = -1;                // update count / the host tree copy's
+    // hit staging for streamed(), page-locked, kept across calls (capacity
+    // from the last count)
+    struct Pinned {
+        void *p = nullptr;
+        ~Pinned() { if (p) mclccd_host_free(p); }
+    };
+    Pinned out_s_, out_v_, out_t_;
     long long out_cap_ = 0;
+    // host copy of the tree for visitors
+    struct HostNode {
+        float l[12], r[12];
+        int d[4], pad[4];
+    };
+    static_assert(sizeof(HostNode) == 128, "node record is 128 bytes");
+    std::vector<HostNode> tree_nodes_;
+    std::vector<double> tree_box_;
+    std::vector<int> tree_prim_;
+    std::vector<unsigned char> tree_flags_;
+
+    void fetch_tree()
+    {
+        if (tree_rev_ == rev_) return;
+        tree_nodes_.resize(np_ > 1 ? np_ - 1 : 0);
+        tree_box_.resize((size_t)np_ * 4 * DIM);
+        tree_prim_.resize(np_);
+        tree_flags_.resize(np_);
+        check(mclccd_get_tree_host(h_, tree_nodes_.data(), tree_box_.data(), tree_prim_.data(), tree_flags_.data()));
+        tree_rev_ = rev_;
+    }
+    // Child `side` of a node as a volume: FP32 t0 / t1 boxes (outward) and
+    // their hull, in T.
+    static BoundingBox<T, DIM> node_volume(const HostNode &nd, int side)
+    {
+        const float *c = side ? nd.r : nd.l;
+        float t0lo[DIM], t0hi[DIM], t1lo[DIM], t1hi[DIM];
+        if constexpr (DIM == 3) {
+            for (int k = 0; k < 3; ++k) { t0lo[k] = c[k]; t1hi[k] = c[9 + k]; }
+            t0hi[0] = c[3]; t0hi[1] = c[4]; t0hi[2] = c[5];
+            t1lo[0] = c[6]; t1lo[1] = c[7]; t1lo[2] = c[8];
+        } else {
+            t0lo[0] = c[0]; t0lo[1] = c[1]; t0hi[0] = c[2]; t0hi[1] = c[3];
+            t1lo[0] = c[4]; t1lo[1] = c[5]; t1hi[0] = c[6]; t1hi[1] = c[7];
+        }
+        BoundingBox<T, DIM> b;
+        for (int k = 0; k < DIM; ++k) {
+            b.t0.min()[k] = (T)t0lo[k]; b.t0.max()[k] = (T)t0hi[k];
+            b.t1.min()[k] = (T)t1lo[k]; b.t1.max()[k] = (T)t1hi[k];
+            b.min()[k] = (T)std::min(t0lo[k], t1lo[k]);
+            b.max()[k] = (T)std::max(t0hi[k], t1hi[k]);
+        }
+        b.active = ((nd.d[1] >> (side ? 16 : 8)) & 0xff) != 0;
+        return b;
+    }
+    // Sorted leaf k as the reference's leaf object (exact FP64 boxes).
+    BVHLeaf<T, DIM> leaf_object(int k) const
+    {
+        BVHLeaf<T, DIM> o;
+        o.idx = tree_prim_[k];
+        const unsigned f = tree_flags_[k];
+        for (int j = 0; j < 3; ++j) {
+            o.v[j] = (f >> j) & 1;
+            o.e[j] = (f >> (3 + j)) & 1;
+        }
+        const double *bx = &tree_box_[(size_t)k * 4 * DIM];   // lo0, hi0, lo1, hi1
+        for (int c = 0; c < DIM; ++c) {
+            o.box.t0.min()[c] = (T)bx[c];
+            o.box.t0.max()[c] = (T)bx[DIM + c];
+            o.box.t1.min()[c] = (T)bx[2 * DIM + c];
+            o.box.t1.max()[c] = (T)bx[3 * DIM + c];
+            o.box.min()[c] = (T)std::min(bx[c], bx[2 * DIM + c]);
+            o.box.max()[c] = (T)std::max(bx[DIM + c], bx[3 * DIM + c]);
+        }
+        o.box.active = (f & (1u << 6)) != 0;
+        return o;
+    }
+    void grow_staging(long long cap)
+    {
+        Pinned s, v, t;
+        check(mclccd_host_alloc(sizeof(int) * 4 * (size_t)cap, &s.p));
+        check(mclccd_host_alloc((size_t)cap, &v.p));
+        check(mclccd_host_alloc(sizeof(double) * (size_t)cap, &t.p));
+        std::swap(out_s_.p, s.p);
+        std::swap(out_v_.p, v.p);
+        std::swap(out_t_.p, t.p);
+        out_cap_ = cap;
+    }
 
     // With only append_pair / append_discrete set: traverse with the hits
     // delivered into host staging (mclccd_traverse_out), so their copy from
@@ -257,20 +470,18 @@ private:
     {
         if (!append_pair || filter_pair || narrow_phase) return false;
         long long nh = 0, nd = 0;
-        check(mclccd_traverse_out(h_, V0, V1, nv_, P, mem_, out_s_.get(), out_v_.get(), out_t_.get(), out_cap_, &nh,
-                                  nullptr, 0, &nd, MCLCCD_MEM_HOST));
+        int *s = static_cast<int *>(out_s_.p);
+        unsigned char *v = static_cast<unsigned char *>(out_v_.p);
+        double *t = static_cast<double *>(out_t_.p);
+        check(mclccd_traverse_out(h_, V0, V1, nv_, P, mem_, s, v, t, out_cap_, &nh, nullptr, 0, &nd, MCLCCD_MEM_HOST));
         if (nh > out_cap_) {
-            const long long cap = nh + nh / 4 + 1024;
-            std::unique_ptr<int[]> s(new int[4 * cap]);
-            std::unique_ptr<unsigned char[]> v(new unsigned char[cap]);
-            std::unique_ptr<double[]> t(new double[cap]);
-            check(mclccd_get_hits(h_, MCLCCD_MEM_HOST, nh, s.get(), v.get(), t.get()));
-            out_s_ = std::move(s);
-            out_v_ = std::move(v);
-            out_t_ = std::move(t);
-            out_cap_ = cap;
+            grow_staging(nh + nh / 4 + 1024);
+            s = static_cast<int *>(out_s_.p);
+            v = static_cast<unsigned char *>(out_v_.p);
+            t = static_cast<double *>(out_t_.p);
+            check(mclccd_get_hits(h_, MCLCCD_MEM_HOST, nh, s, v, t));
         }
-        for (long long i = 0; i < nh; ++i) append_pair(make_stencil(&out_s_[4 * i]), out_v_[i] != 0, to_toi(out_t_[i]));
+        for (long long i = 0; i < nh; ++i) append_pair(make_stencil(&s[4 * i]), v[i] != 0, to_toi(t[i]));
         dispatch_discrete();
         return true;
     }

@@ -231,11 +231,11 @@ class BVHTree:
         self.precision = precision
 
     TUNE_KEYS = {"expand_grid": 0, "accd_grid": 1, "walk_packet": 2, "accd_rebin": 3, "walk_window": 4, "overlap": 5,
-                 "narrow_fused": 6, "fused_grid": 7}
+                 "narrow_fused": 6, "fused_grid": 7, "walk_refill": 8}
 
     def set_tuning(self, **kv):
         """Launch-shape knobs (expand_grid, accd_grid, walk_packet, accd_rebin, walk_window, overlap,
-        narrow_fused, fused_grid); results never depend on them."""
+        narrow_fused, fused_grid, walk_refill); results never depend on them."""
         for k, v in kv.items():
             self._check(self._L.mclccd_set_tuning(self._h, self.TUNE_KEYS[k], int(v)), self._h)
 

@@ -307,6 +307,23 @@ void launch_owner_flags(const int *P, int np, int pdim, int nv, int *vowner, uns
     k_owner_flags<<<(np + 255) / 256, 256, 0, st>>>(P, np, pdim, nv, vowner, ekeys, eowner, ecap - 1, flags);
 }
 
+// out = max(out, 1 + the largest entry of a[0..n)): the vertex count implied
+// by a primitive array.
+__global__ void k_max_index(const int *__restrict__ a, long long n, int *out)
+{
+    int m = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = max(m, __ldg(a + i) + 1);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane_id() == 0 && m > 0) atomicMax(out, m);
+}
+
+void launch_max_index(const int *a, long long n, int *out, cudaStream_t st)
+{
+    k_max_index<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(a, n, out);
+}
+
 void launch_compare(const int *a, const int *b, long long n, int *diff, cudaStream_t st)
 {
     long long n4 = n / 4;

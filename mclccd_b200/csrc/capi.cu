@@ -67,12 +67,13 @@ struct mclccd_tree {
     DevBuf pairs, vf, ee, hit_sten, hit_toi, hit_isvf, disc, counters, diff, fp64_queue;
     DevBuf in_V, in_P, in_act, in_tmp;   // input conversion staging (mclccd_update_ex / mclccd_traverse_ex)
     DevBuf cand_cnt;                     // counters of the on-request candidate expansion
+    DevBuf walk_cursor;                  // query cursor of the refill walk
     std::vector<DevBuf *> all()
     {
         return {&V0d, &V1d, &Pd, &Pstage, &actd, &pflags, &pflags_tmp, &vowner, &ekeys, &eowner, &cent, &bounds,
                 &keys, &vals, &keys_alt, &vals_alt, &sort_scratch, &nodes, &leaf_parent, &visits, &leaf_box,
                 &leaf_active, &pairs, &vf, &ee, &hit_sten, &hit_toi, &hit_isvf, &disc, &counters, &diff,
-                &fp64_queue, &in_V, &in_P, &in_act, &in_tmp, &cand_cnt};
+                &fp64_queue, &in_V, &in_P, &in_act, &in_tmp, &cand_cnt, &walk_cursor};
     }
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
@@ -88,7 +89,7 @@ struct mclccd_tree {
     cudaEvent_t out_ev[16] = {};
     unsigned long long *h_snap = nullptr;
     unsigned long long out_done = 0;   // hits already copied out by the streamed path
-    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0, 0, kFusedGrid};
+    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0, 0, kFusedGrid, 0};
     // The fused narrow phase counts the candidate lists without writing them;
     // mclccd_get_candidates rebuilds them from the leaf pairs and the P of the
     // last traverse.
@@ -152,6 +153,24 @@ int device_errors(mclccd_tree *t, unsigned err)
 }
 
 } // namespace
+
+// The tree walk over queries [qb, qe) (qe < 0: all): the refill form when
+// tuned in (and not the packet walk), else launch_traverse's forms.
+static int launch_walk(mclccd_tree *t, int dim, int packet, int np, Counters *cnt, cudaStream_t st, int qb = 0,
+                       int qe = -1)
+{
+    if (!packet && t->tune[MCLCCD_TUNE_WALK_REFILL]) {
+        MC_CUDA(t, ensure(t->walk_cursor, sizeof(unsigned)));
+        launch_traverse_refill(dim, t->tune[MCLCCD_TUNE_WALK_WINDOW] ? t->tune[MCLCCD_TUNE_WALK_WINDOW] : 16,
+                               as<Node>(t->nodes), t->leaf_box.p, as<unsigned char>(t->leaf_active), as<int>(t->vals),
+                               np, as<int2>(t->pairs), t->cap_pairs, cnt, as<unsigned>(t->walk_cursor), st, qb, qe);
+        return MCLCCD_OK;
+    }
+    launch_traverse(dim, packet, t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes), t->leaf_box.p,
+                    as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs, cnt, st,
+                    qb, qe);
+    return MCLCCD_OK;
+}
 
 // Inputs in other forms than row-major double (float coordinates, column-
 // major V or P): one pass converts them on the device into the row-major
@@ -261,9 +280,7 @@ static int enqueue_overlapped(mclccd_tree *t, int chunks, int dim, int np, int n
     const int nq = np - 1;
     for (int c = 0; c < chunks; ++c) {
         const int qb = (int)((long long)nq * c / chunks), qe = (int)((long long)nq * (c + 1) / chunks);
-        launch_traverse(dim, 0, t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes), t->leaf_box.p,
-                        as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
-                        cnt, t->s_walk, qb, qe);
+        if (int rc = launch_walk(t, dim, 0, np, cnt, t->s_walk, qb, qe)) return rc;
         launch_snapshot(&cnt->n_pairs, pe + c + 1, nullptr, nullptr, t->s_walk);
         MC_CUDA(t, cudaEventRecord(t->ov_ev[1], t->s_walk));
         MC_CUDA(t, cudaStreamWaitEvent(t->s_narrow, t->ov_ev[1], 0));
@@ -329,9 +346,7 @@ static int enqueue_streamed(mclccd_tree *t, int dim, int np, int nv, const int *
     const int nq = np - 1;
     for (int c = 0; c < kOutChunks; ++c) {
         const int qb = (int)((long long)nq * c / kOutChunks), qe = (int)((long long)nq * (c + 1) / kOutChunks);
-        launch_traverse(dim, 0, t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes), t->leaf_box.p,
-                        as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs,
-                        cnt, st, qb, qe);
+        if (int rc = launch_walk(t, dim, 0, np, cnt, st, qb, qe)) return rc;
         launch_snapshot(&cnt->n_pairs, pe + c + 1, nullptr, nullptr, st);
         if (fused) {
             launch_narrow_fused(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV0, dV1, nv,
@@ -433,10 +448,10 @@ int mclccd_create(int dim, mclccd_tree **out)
     cudaError_t e = cudaGetDevice(&t->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&t->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&t->h_cnt, sizeof(Counters));
-    if (e == cudaSuccess) e = cudaMallocHost(&t->h_diff, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&t->h_diff, 2 * sizeof(int));
     for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&t->ev[i]);
     if (e == cudaSuccess) e = ensure(t->counters, sizeof(Counters));
-    if (e == cudaSuccess) e = ensure(t->diff, sizeof(int));
+    if (e == cudaSuccess) e = ensure(t->diff, 2 * sizeof(int));
     if (e != cudaSuccess) {
         mclccd_destroy(t);
         return e == cudaErrorMemoryAllocation ? MCLCCD_ERR_NOMEM : MCLCCD_ERR_CUDA;
@@ -528,13 +543,38 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
         t->flags_np = 0;
         return MCLCCD_OK;
     }
-    if (!V0 || !V1 || !P || nv <= 0) return fail(t, MCLCCD_ERR_INVALID, "null array or nv == 0");
+    if (!V0 || !V1 || !P || nv < 0) return fail(t, MCLCCD_ERR_INVALID, "null array or nv < 0");
     if (pdim < 1 || pdim > 4) return fail(t, MCLCCD_ERR_INVALID, "pdim must be in [1, 4]");
     DeviceGuard g(t->device);
     cudaStream_t st = t->stream;
     const int dim = t->dim;
     const bool prof = (t->flags & MCLCCD_OPT_PROFILE) != 0;
     if (prof) cudaEventRecord(t->ev[0], st);
+    const long long pcount = (long long)np * pdim;
+    MC_CUDA(t, ensure(t->Pstage, sizeof(int) * (size_t)pcount));
+    // Refit-only when the topology is byte-identical to the previous update.
+    const bool may_refit = t->built && t->np > 1 && !(t->flags & MCLCCD_OPT_ALWAYS_REBUILD) && np == t->np &&
+                           pdim == t->pdim;
+    int p_known = -1;   // -1: P not compared yet; 0 / 1: P differs / equals the stored P
+    const bool derive_nv = nv == 0;
+    if (derive_nv) {
+        // The reference's update carries no vertex count: it is 1 + the
+        // largest index in P, found on the device (with the refit check's
+        // compare, one small read-back).
+        MC_CUDA(t, cudaMemcpyAsync(t->Pstage.p, P, sizeof(int) * (size_t)pcount, h2d_or_d2d(mem_kind), st));
+        MC_CUDA(t, cudaMemsetAsync(t->diff.p, 0, 2 * sizeof(int), st));
+        launch_max_index(as<int>(t->Pstage), pcount, as<int>(t->diff) + 1, st);
+        ++t->launches;
+        if (may_refit) {
+            launch_compare(as<int>(t->Pstage), as<int>(t->Pd), pcount, as<int>(t->diff), st);
+            ++t->launches;
+        }
+        MC_CUDA(t, cudaMemcpyAsync(t->h_diff, t->diff.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        MC_CUDA(t, cudaStreamSynchronize(st));
+        nv = t->h_diff[1];
+        if (nv <= 0) return fail(t, MCLCCD_ERR_INVALID, "nv == 0 and P holds no vertex index >= 0");
+        if (may_refit) p_known = t->h_diff[0] == 0 ? 1 : 0;
+    }
 
     const double *dV0 = V0, *dV1 = V1;
     const int *dact = active;
@@ -552,15 +592,14 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
             dact = as<int>(t->actd);
         }
     }
-    const long long pcount = (long long)np * pdim;
-    MC_CUDA(t, ensure(t->Pstage, sizeof(int) * (size_t)pcount));
-    MC_CUDA(t, cudaMemcpyAsync(t->Pstage.p, P, sizeof(int) * (size_t)pcount, h2d_or_d2d(mem_kind), st));
+    if (!derive_nv)
+        MC_CUDA(t, cudaMemcpyAsync(t->Pstage.p, P, sizeof(int) * (size_t)pcount, h2d_or_d2d(mem_kind), st));
     MC_CUDA(t, cudaMemsetAsync(t->counters.p, 0, sizeof(Counters), st));
 
-    // Refit-only when the topology is byte-identical to the previous update.
-    bool same = t->built && t->np > 1 && !(t->flags & MCLCCD_OPT_ALWAYS_REBUILD) && np == t->np &&
-                pdim == t->pdim && nv == t->nv;
-    if (same) {
+    bool same = may_refit && nv == t->nv;
+    if (same && p_known >= 0) {
+        same = p_known == 1;
+    } else if (same) {
         MC_CUDA(t, cudaMemsetAsync(t->diff.p, 0, sizeof(int), st));
         launch_compare(as<int>(t->Pstage), as<int>(t->Pd), pcount, as<int>(t->diff), st);
         ++t->launches;
@@ -841,9 +880,7 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
         } else if (chunks >= 2 && cont && !certified && !t->tune[MCLCCD_TUNE_WALK_PACKET] && np > 2 * chunks * 128) {
             if (int rc = enqueue_overlapped(t, chunks, dim, np, nv, dP, dV0, dV1, discr, fused, cnt, accd)) return rc;
         } else {
-            launch_traverse(dim, t->tune[MCLCCD_TUNE_WALK_PACKET], t->tune[MCLCCD_TUNE_WALK_WINDOW],
-                            as<Node>(t->nodes), t->leaf_box.p, as<unsigned char>(t->leaf_active), as<int>(t->vals), np,
-                            as<int2>(t->pairs), t->cap_pairs, cnt, st);
+            if (int rc = launch_walk(t, dim, t->tune[MCLCCD_TUNE_WALK_PACKET], np, cnt, st)) return rc;
             if (prof) cudaEventRecord(t->ev[4], st);
             if (fused) {   // expansion, discrete test and ACCD in one kernel: "expand" reads 0
                 if (prof) cudaEventRecord(t->ev[5], st);
@@ -1274,6 +1311,72 @@ int mclccd_get_tree_view(const mclccd_tree *t, mclccd_tree_view *view)
     return MCLCCD_OK;
 }
 
+int mclccd_get_tree_host(mclccd_tree *t, void *nodes, double *leaf_box, int *leaf_prim, unsigned char *leaf_flags)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!t->built || t->np < 1) return fail(t, MCLCCD_ERR_STATE, "no tree: update first");
+    DeviceGuard g(t->device);
+    const int np = t->np, dim = t->dim;
+    cudaStream_t st = t->stream;
+    if (nodes && np > 1)
+        MC_CUDA(t, cudaMemcpyAsync(nodes, t->nodes.p, sizeof(Node) * (size_t)(np - 1), cudaMemcpyDeviceToHost, st));
+    if (leaf_box)
+        MC_CUDA(t, cudaMemcpyAsync(leaf_box, t->leaf_box.p, sizeof(double) * 4 * dim * (size_t)np,
+                                   cudaMemcpyDeviceToHost, st));
+    std::vector<int> sorted;
+    int *prim = leaf_prim;
+    if (!prim && leaf_flags) {
+        sorted.resize(np);
+        prim = sorted.data();
+    }
+    if (prim) MC_CUDA(t, cudaMemcpyAsync(prim, t->vals.p, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, st));
+    std::vector<unsigned char> act, fl;
+    if (leaf_flags) {
+        act.resize(np);
+        fl.resize(np);
+        MC_CUDA(t, cudaMemcpyAsync(act.data(), t->leaf_active.p, np, cudaMemcpyDeviceToHost, st));
+        MC_CUDA(t, cudaMemcpyAsync(fl.data(), t->pflags.p, np, cudaMemcpyDeviceToHost, st));
+    }
+    MC_CUDA(t, cudaStreamSynchronize(st));
+    if (leaf_flags)
+        for (int k = 0; k < np; ++k)
+            leaf_flags[k] = (unsigned char)((fl[prim[k]] & kFlagAllRep) | (act[k] ? kFlagActive : 0));
+    return MCLCCD_OK;
+}
+
+int mclccd_tree_size(const mclccd_tree *t, int *nv, int *np, int *pdim)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (!t->built) return MCLCCD_ERR_STATE;
+    if (nv) *nv = t->nv;
+    if (np) *np = t->np;
+    if (pdim) *pdim = t->pdim;
+    return MCLCCD_OK;
+}
+
+int mclccd_host_alloc(size_t bytes, void **ptr)
+{
+    if (!ptr) return MCLCCD_ERR_INVALID;
+    *ptr = nullptr;
+    if (bytes == 0) return MCLCCD_OK;
+    const cudaError_t e = cudaHostAlloc(ptr, bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
+        return e == cudaErrorMemoryAllocation ? MCLCCD_ERR_NOMEM : MCLCCD_ERR_CUDA;
+    }
+    return MCLCCD_OK;
+}
+
+int mclccd_host_free(void *ptr)
+{
+    if (ptr && cudaFreeHost(ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return MCLCCD_ERR_CUDA;
+    }
+    return MCLCCD_OK;
+}
+
 int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)
 {
     if (!t || !ms || n < 0) return -1;
@@ -1285,12 +1388,18 @@ int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)
 int mclccd_set_tuning(mclccd_tree *t, int key, int value)
 {
     if (!t || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
-    const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_ACCD_REBIN || key == MCLCCD_TUNE_NARROW_FUSED;
+    const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_ACCD_REBIN ||
+                      key == MCLCCD_TUNE_NARROW_FUSED || key == MCLCCD_TUNE_WALK_REFILL;
     if (key == MCLCCD_TUNE_OVERLAP) {
         if (value < 0 || value > 16) return fail(t, MCLCCD_ERR_INVALID, "overlap chunks must be in [0, 16]");
     } else if (key == MCLCCD_TUNE_WALK_WINDOW) {
         if (value != 0 && value != 8 && value != 16 && value != 32 && value != 64 && value != 128)
             return fail(t, MCLCCD_ERR_INVALID, "walk window must be 0, 8, 16, 32, 64 or 128");
+        if (t->tune[MCLCCD_TUNE_WALK_REFILL] && (value == 0 || value > 32))
+            return fail(t, MCLCCD_ERR_INVALID, "the refill walk takes a window of 8, 16 or 32");
+    } else if (key == MCLCCD_TUNE_WALK_REFILL && value == 1 &&
+               (t->tune[MCLCCD_TUNE_WALK_WINDOW] == 0 || t->tune[MCLCCD_TUNE_WALK_WINDOW] > 32)) {
+        return fail(t, MCLCCD_ERR_INVALID, "the refill walk takes a window of 8, 16 or 32");
     } else if (flag ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))
         return fail(t, MCLCCD_ERR_INVALID, "tuning value out of range");
     t->tune[key] = value;

@@ -17,6 +17,7 @@ void launch_refit(int dim, const double *V0, const double *V1, const int *P, int
 void launch_owner_flags(const int *P, int np, int pdim, int nv, int *vowner, unsigned long long *ekeys, int *eowner,
                         unsigned long long ecap, unsigned char *flags, Counters *cnt, cudaStream_t st);
 void launch_compare(const int *a, const int *b, long long n, int *diff, cudaStream_t st);
+void launch_max_index(const int *a, long long n, int *out, cudaStream_t st);
 
 // sort.cu
 int sort_num_passes(unsigned key_bits);
@@ -29,6 +30,12 @@ void launch_sort_pairs(unsigned *keys, int *vals, unsigned *keys_alt, int *vals_
 void launch_traverse(int dim, int packet, int window, const Node *nodes, const void *leaf_box, const unsigned char *leaf_active,
                      const int *sorted, int n, int2 *pairs, unsigned long long cap, Counters *cnt, cudaStream_t st,
                      int q_begin = 0, int q_end = -1);
+// the window walk with idle lanes refilled from a per-warp pool of queries
+// (persistent; cursor: one device unsigned, zeroed by the launcher)
+void launch_traverse_refill(int dim, int window, const Node *nodes, const void *leaf_box,
+                            const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs,
+                            unsigned long long cap, Counters *cnt, unsigned *cursor, cudaStream_t st,
+                            int q_begin = 0, int q_end = -1);
 void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,
                          const unsigned char *flags, const double *V1, int nv, int4 *vf, unsigned long long vf_cap,
                          int4 *ee, unsigned long long ee_cap, int2 *disc, unsigned long long disc_cap, int continuous,

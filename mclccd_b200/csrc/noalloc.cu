@@ -33,7 +33,9 @@ static __device__ __align__(256) unsigned char g_static_scratch[kScratchBytes];
 
 // Device address of g_static_scratch per device.  In host code the symbol is
 // only a host-side stand-in, so the address is looked up with
-// cudaGetSymbolAddress once per device, with that device current.
+// cudaGetSymbolAddress once per device, with that device current, and kept
+// for the life of the process: a reset of the device's primary context
+// (cudaDeviceReset) would leave it stale, which the header documents.
 std::mutex g_mu;
 void *g_addr[kMaxDevices] = {};
 

@@ -10,6 +10,8 @@
 // exactly the reference's.  Pairs are emitted canonically (lower primitive
 // index first).
 #include "common.cuh"
+
+#include <algorithm>
 #include "geom.cuh"
 #include "kernels.cuh"
 #include "lbvh.cuh"
@@ -219,6 +221,164 @@ k_traverse_window(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// Refill form (MCLCCD_TUNE_WALK_REFILL): the window walk with idle lanes
+// refilled.  In the plain walk a warp runs until its slowest query is done,
+// so most lanes idle through the long walks (about a third of the lanes are
+// active per instruction).  Here each warp is persistent: it takes chunks of
+// 32 consecutive queries from a global cursor, runs their window part (the
+// W leaves after each query, staged per warp in shared memory: coherent) and
+// queues them for the tree part in a per-warp pool; lanes whose tree walk is
+// done take the next query from the pool, and the warp fetches a new chunk
+// when the pool runs dry while a lane is idle.  Every query tests the same
+// leaves with the same three-valued test and FP64 fallback as the window
+// form, so the leaf-pair set is the same; only the order of the pairs in the
+// list differs.
+// ---------------------------------------------------------------------------
+template <int DIM, int W>
+__global__ void __launch_bounds__(128, 4)
+k_traverse_refill(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
+                  const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n, int q_begin,
+                  int q_end, int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt,
+                  unsigned *__restrict__ cursor)
+{
+    constexpr int S = DIM == 3 ? 3 : 2;
+    constexpr int NB = 32 + W;     // staged leaves per chunk: base + 1 .. base + 32 + W
+    constexpr int POOL = 64;       // queries waiting for their tree part (< 32 left + one chunk)
+    __shared__ float s_box[4][NB][4 * DIM];   // t0lo, t0hi, t1lo, t1hi (outward FP32)
+    __shared__ unsigned char s_act[4][NB];
+    __shared__ int s_pool[4][POOL];
+    __shared__ int stack[kStackDepth][128];
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const unsigned full = 0xffffffffu;
+
+    // leaf k against query qi (box qb, primitive qp): three-valued FP32 test,
+    // FP64 boxes when it cannot tell
+    auto leaf = [&](int qi, const Box2T<DIM> &qb, int qp, int k, const Box2T<DIM> &kb) {
+        int r = leaf_test3<DIM>(qb, inner<DIM>(qb), kb);
+        if (r == 2) r = leaf_boxes_intersect<DIM>(leaf_box[qi], leaf_box[k]) ? 1 : 0;
+        if (r == 1) {
+            const int kp = __ldg(sorted + k);
+            const unsigned long long slot = warp_append(&cnt->n_pairs);
+            if (slot < cap) pairs[slot] = make_int2(min(qp, kp), max(qp, kp));
+        }
+    };
+
+    int npool = 0;            // warp-uniform
+    bool exhausted = false;   // warp-uniform
+    int q = -1, qw = 0, qprim = 0, node = 0, sp = 0, steps = 0;
+    bool qact = false;
+    Box2T<DIM> qbox;
+    for (;;) {
+        const unsigned idle = __ballot_sync(full, q < 0);
+        if (idle && npool == 0 && !exhausted) {
+            // next chunk: its window part, then into the pool
+            unsigned b = 0;
+            if (lane == 0) b = atomicAdd(cursor, 32u);
+            b = __shfl_sync(full, b, 0);
+            const long long base = (long long)q_begin + b;
+            if (base >= q_end) {
+                exhausted = true;
+                continue;
+            }
+            for (int i = lane; i < NB; i += 32) {
+                const long long k = base + 1 + i;
+                if (k < n) {
+                    const Box2T<DIM> kb = outward<DIM>(leaf_box[k]);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        s_box[w][i][d] = kb.t0lo[d];
+                        s_box[w][i][DIM + d] = kb.t0hi[d];
+                        s_box[w][i][2 * DIM + d] = kb.t1lo[d];
+                        s_box[w][i][3 * DIM + d] = kb.t1hi[d];
+                    }
+                    s_act[w][i] = leaf_active[k];
+                }
+            }
+            __syncwarp();
+            const int cq = (int)base + lane;
+            const bool valid = base + lane < q_end;
+            if (valid) {
+                const Box2T<DIM> cb = outward<DIM>(leaf_box[cq]);
+                const bool cact = leaf_active[cq] != 0;
+                const int cp = sorted[cq];
+                const int cw = min(cq + W, n - 1);
+                for (int k = cq + 1; k <= cw; ++k) {
+                    const int i = k - (int)base - 1;
+                    if (!(cact || s_act[w][i])) continue;
+                    Box2T<DIM> kb;
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        kb.t0lo[d] = s_box[w][i][d]; kb.t0hi[d] = s_box[w][i][DIM + d];
+                        kb.t1lo[d] = s_box[w][i][2 * DIM + d]; kb.t1hi[d] = s_box[w][i][3 * DIM + d];
+                    }
+                    leaf(cq, cb, cp, k, kb);
+                }
+            }
+            const unsigned vm = __ballot_sync(full, valid);
+            if (valid) s_pool[w][npool + __popc(vm & lanemask_lt())] = cq;
+            npool += __popc(vm);
+            __syncwarp();
+            continue;
+        }
+        if (idle && npool > 0) {   // idle lanes take queries from the pool
+            const int take = min(__popc(idle), npool);
+            const int rank = __popc(idle & lanemask_lt());
+            if (q < 0 && rank < take) {
+                q = s_pool[w][npool - 1 - rank];
+                qbox = outward<DIM>(leaf_box[q]);
+                qact = leaf_active[q] != 0;
+                qprim = sorted[q];
+                qw = min(q + W, n - 1);
+                node = 0;
+                sp = 0;
+                steps = 0;
+            }
+            npool -= take;
+            __syncwarp();
+        }
+        if (__ballot_sync(full, q >= 0) == 0) {
+            if (exhausted && npool == 0) break;
+            continue;
+        }
+        if (q < 0) continue;
+        // one node of this lane's tree walk (leaves beyond its window)
+        if (++steps > n) {
+            atomicOr(&cnt->err, kErrStack);
+            q = -1;
+            continue;
+        }
+        float4 ls[S], rs[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) { ls[i] = __ldg(&nodes[node].l[i]); rs[i] = __ldg(&nodes[node].r[i]); }
+        const int4 d = __ldg(&nodes[node].d);
+        const int split = d.x, meta = d.y, last = d.z;
+        Box2T<DIM> lb, rb;
+        unpack_child<DIM>(ls, lb);
+        unpack_child<DIM>(rs, rb);
+        const bool lact = ((meta >> 8) & 0xff) != 0, ract = ((meta >> 16) & 0xff) != 0;
+        bool lok = split > qw && (qact || lact);
+        bool rok = last > qw && (qact || ract);
+        if (lok && (meta & kMetaLeftLeaf)) { leaf(q, qbox, qprim, split, lb); lok = false; }
+        if (rok && (meta & kMetaRightLeaf)) { leaf(q, qbox, qprim, split + 1, rb); rok = false; }
+        lok = lok && boxes_may_intersect<DIM>(qbox, lb);
+        rok = rok && boxes_may_intersect<DIM>(qbox, rb);
+        if (lok) {
+            if (rok) {
+                if (sp < kStackDepth) stack[sp++][tid] = split + 1;
+                else atomicOr(&cnt->err, kErrStack);
+            }
+            node = split;
+        } else if (rok) {
+            node = split + 1;
+        } else if (sp == 0) {
+            q = -1;
+        } else {
+            node = stack[--sp][tid];
+        }
+    }
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(128)
 k_traverse_packet(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
@@ -379,6 +539,39 @@ k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, cons
             }
         }
     }
+}
+
+void launch_traverse_refill(int dim, int window, const Node *nodes, const void *leaf_box,
+                            const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs,
+                            unsigned long long cap, Counters *cnt, unsigned *cursor, cudaStream_t st, int q_begin,
+                            int q_end)
+{
+    if (n < 2) return;
+    if (q_end < 0 || q_end > n - 1) q_end = n - 1;
+    if (q_begin >= q_end) return;
+    // persistent: one wave of resident blocks, fewer for short ranges
+    const long long warps_needed = ((long long)(q_end - q_begin) + 31) / 32;
+    const int g = (int)std::max<long long>(1, std::min<long long>(148 * 4, (warps_needed + 3) / 4));
+    cudaMemsetAsync(cursor, 0, sizeof(unsigned), st);
+    const auto *lb3 = reinterpret_cast<const LeafBox<3> *>(leaf_box);
+    const auto *lb2 = reinterpret_cast<const LeafBox<2> *>(leaf_box);
+#define MCLCCD_REFILL_CASE(Wv)                                                                                     \
+    case Wv:                                                                                                       \
+        if (dim == 3)                                                                                              \
+            k_traverse_refill<3, Wv><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, q_begin, q_end, pairs,  \
+                                                         cap, cnt, cursor);                                         \
+        else                                                                                                       \
+            k_traverse_refill<2, Wv><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, q_begin, q_end, pairs,  \
+                                                         cap, cnt, cursor);                                         \
+        return;
+    // (the per-warp staging of 32 + W boxes keeps W <= 32 within static shared memory)
+    switch (window) {
+        MCLCCD_REFILL_CASE(8)
+        MCLCCD_REFILL_CASE(32)
+    default:
+        MCLCCD_REFILL_CASE(16)
+    }
+#undef MCLCCD_REFILL_CASE
 }
 
 void launch_traverse(int dim, int packet, int window, const Node *nodes, const void *leaf_box,

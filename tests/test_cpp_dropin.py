@@ -101,3 +101,56 @@ def test_dropin_float_tree(tmp_path):
     print(f"float tree: {len(got)} hits; reference float instantiation {len(rt)} hits, same set {same}, "
           f"max rel toi difference {rel:.2e}")
     assert len(common) >= 0.999 * max(len(rt), len(got))
+
+
+def build_cpp(tmp_path, name):
+    exe = str(tmp_path / name)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", name + ".cpp"), "-L", LIBDIR, "-lmclccd_b200",
+                    f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
+    return exe
+
+
+def test_visitor_program_compiles(tmp_path):
+    assert os.path.exists(build_cpp(tmp_path, "traverser_main"))
+
+
+def point_in_triangle_brute(V, F, Q):
+    a, b, c = V[F[:, 0]], V[F[:, 1]], V[F[:, 2]]
+    v0, v1 = b - a, c - a
+    d00, d01, d11 = (v0 * v0).sum(1), (v0 * v1).sum(1), (v1 * v1).sum(1)
+    out = []
+    for p in Q:
+        v2 = p - a
+        d20, d21 = (v2 * v0).sum(1), (v2 * v1).sum(1)
+        inv = 1.0 / (d00 * d11 - d01 * d01)
+        s, t = (d11 * d20 - d01 * d21) * inv, (d00 * d21 - d01 * d20) * inv
+        out.append(sorted(np.flatnonzero((s >= 0) & (t >= 0) & (1.0 - s - t >= 0)).tolist()))
+    return out
+
+
+@pytest.mark.gpu
+def test_visitor_point_in_triangle_matches_brute_force(tmp_path):
+    # BVHTree<double, 2>::traverse(BVHTraverse *) driven like the reference's
+    # examples/traverser.cpp: every query finds exactly the triangles whose
+    # barycentric test passes (the visitor descends into volumes containing
+    # the point and checks each leaf it reaches)
+    from mclccd_b200 import scenes
+    exe = build_cpp(tmp_path, "traverser_main")
+    V3, _, F, _ = scenes.folded_cloth(48, seed=3)
+    rng = np.random.default_rng(5)
+    V = np.ascontiguousarray(V3[:, :2] + rng.normal(0, 2e-3, (len(V3), 2)))
+    Q = np.concatenate([rng.uniform(-0.05, 1.05, (400, 2)), V[rng.choice(len(V), 50)]])   # vertices: ties
+    scene = tmp_path / "scene.bin"
+    with open(scene, "wb") as f:
+        f.write(np.array([len(V), len(F), len(Q)], np.int32).tobytes())
+        f.write(V.tobytes()); f.write(F.astype(np.int32).tobytes()); f.write(Q.tobytes())
+    out = tmp_path / "out.bin"
+    subprocess.run([exe, str(scene), str(out)], check=True)
+    raw = np.frombuffer(out.read_bytes(), np.int32)
+    got, i = [], 0
+    for _ in range(len(Q)):
+        n = int(raw[i]); got.append(sorted(raw[i + 1:i + 1 + n].tolist())); i += 1 + n
+    want = point_in_triangle_brute(V, F.astype(np.int64), Q)
+    assert got == want
+    assert sum(len(w) for w in want) > 300

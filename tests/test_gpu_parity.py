@@ -208,6 +208,74 @@ def test_walk_window_against_port(port, window, scene):
     check_against_port(t, port, V0, V1, F, eta)
 
 
+def device_results(t):
+    cs, cv = t.candidates()
+    return canonical_set(cs, cv), hit_map(*t.hits()), sort_rows(t.discrete())
+
+
+@pytest.mark.parametrize("window", [8, 16, 32])
+@pytest.mark.parametrize("scene", ["wavy", "annulus", "active"])
+def test_walk_refill_matches_window_walk(window, scene):
+    # the refill walk (persistent warps, idle lanes refilled from a per-warp
+    # query pool) finds the same leaf pairs as the window walk it reorders;
+    # candidates, hits with toi and discrete pairs equal, in the full step and
+    # in the streamed (query-chunked) step
+    torch = pytest.importorskip("torch")
+    V0, V1, F, eta = scenes.wavy_cloth(1025, rows=97, seed=5) if scene != "annulus" else scenes.annulus_2d(500, seed=6)
+    act = (np.arange(len(V0)) % 7 < 2).astype(np.int32) if scene == "active" else None
+    out = []
+    for refill in (0, 1):
+        t = BVHTree(V0.shape[1])
+        t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+        t.set_tuning(walk_window=window)
+        t.set_tuning(walk_refill=refill)
+        t.update(V0, V1, F, active=act)
+        t.traverse(V0, V1, F)
+        out.append(device_results(t) + (t.counts()["leaf_pairs"],))
+    assert out[0][3] == out[1][3] > 0
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
+    if scene == "wavy":   # chunked queries through traverse_out
+        n = len(out[0][1])
+        hs = torch.empty((n + 64, 4), dtype=torch.int32).pin_memory()
+        hv = torch.empty(n + 64, dtype=torch.uint8).pin_memory()
+        ht = torch.empty(n + 64, dtype=torch.float64).pin_memory()
+        nh, _ = t.traverse_out(hs, hv, ht)
+        assert nh == n and hit_map(hs[:n].numpy(), hv[:n].numpy(), ht[:n].numpy()) == out[0][1]
+
+
+@pytest.mark.parametrize("scene", ["fold", "annulus", "wavy"])
+def test_fused_narrow_phase_against_port(port, scene):
+    # the fused form (pairs -> stencils -> discrete test -> ACCD in one
+    # kernel, candidate lists rebuilt on request) gives the reference's sets
+    if scene == "fold":
+        V0, V1, F, eta = scenes.folded_cloth(40, seed=8)
+    elif scene == "annulus":
+        V0, V1, F, eta = scenes.annulus_2d(300, seed=9)
+    else:
+        V0, V1, F, eta = scenes.wavy_cloth(1025, rows=49, seed=3)
+    t = BVHTree(V0.shape[1])
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.set_tuning(narrow_fused=1)
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    check_against_port(t, port, V0, V1, F, eta)
+    c = t.counts()
+    p = port.run(V0, V1, F, eta)
+    assert (c["vf"], c["ee"]) == (int(p["cand_is_vf"].sum()), int(len(p["cand_is_vf"]) - p["cand_is_vf"].sum()))
+
+
+def test_walk_refill_against_port(port):
+    V0, V1, F, eta = scenes.folded_cloth(40, seed=7)
+    t = BVHTree(3)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.set_tuning(walk_refill=1)
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    check_against_port(t, port, V0, V1, F, eta)
+
+
 @pytest.mark.parametrize("dim", [3, 2])
 def test_rebinned_accd_against_port(port, dim):
     # the re-binned ACCD form (heads and tails in separate warp passes) gives
