@@ -72,6 +72,10 @@ int mclccd_create(int dim, mclccd_tree **out);
 /* Replaces: ~BVHTree().  Frees every device buffer the handle owns. */
 int mclccd_destroy(mclccd_tree *tree);
 
+/* Full hierarchy builds since creation, and how many of them the tree-
+ * quality trigger (MCLCCD_TUNE_REBUILD_RATIO) caused. */
+int mclccd_build_stats(const mclccd_tree *tree, long long *builds, long long *quality_rebuilds);
+
 /* Sizes of the last update: vertex count (the derived one when the update
  * passed nv = 0), primitive count and primitive width (any may be NULL). */
 int mclccd_tree_size(const mclccd_tree *tree, int *nv, int *np, int *pdim);
@@ -365,8 +369,9 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
  * blocks) of the stencil-expansion kernel and of the ACCD kernels, the
  * tree-walk form (1: warp-cooperative packets, 0: one query per thread) and
  * the FP64 ACCD form (1: stencils that go on after the first distance are
- * re-binned in shared memory so warps run heads or tails, never both; 0, the
- * default and faster on B200: one stencil per thread start to end), and the
+ * re-binned in shared memory so warps run heads or tails, never both; 2: the
+ * head in one kernel over the list, the tail in a second over a queue of the
+ * stencils that go on; 0: one stencil per thread start to end), and the
  * walk's Morton window (W = 8, 16 (default), 32, 64 or 128: each query
  * first tests the W leaves after it in Morton order, staged by its block in
  * shared memory, then walks the tree only for leaves beyond them; 0: tree
@@ -382,7 +387,15 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
  * 32 queries, run their window part, and refill lanes whose tree walk is
  * done from a per-warp pool of queries, so lanes do not idle behind the
  * longest walk of their warp; window 8, 16 or 32; 0: one query per thread
- * start to end).  Results do not depend on any of them. */
+ * start to end), the expansion split (1: the stencil expansion and the
+ * discrete test as two kernels; 0: one kernel), and the rebuild ratio (in
+ * percent; default 150): every refit sums the box areas of the internal
+ * nodes relative to those of the leaves, and when that grows past the ratio
+ * of its value after the last full build, the next update rebuilds the
+ * hierarchy (0: refit whenever P is unchanged), and the buffered walk (1:
+ * the window walk collects each warp's leaf pairs in shared memory and
+ * writes them 32 at a time with one atomic; window 8, 16 or 32).  Results do
+ * not depend on any of them. */
 #define MCLCCD_TUNE_EXPAND_GRID 0
 #define MCLCCD_TUNE_ACCD_GRID 1
 #define MCLCCD_TUNE_WALK_PACKET 2
@@ -392,7 +405,10 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
 #define MCLCCD_TUNE_NARROW_FUSED 6
 #define MCLCCD_TUNE_FUSED_GRID 7
 #define MCLCCD_TUNE_WALK_REFILL 8
-#define MCLCCD_TUNE_COUNT 9
+#define MCLCCD_TUNE_EXPAND_SPLIT 9
+#define MCLCCD_TUNE_REBUILD_RATIO 10
+#define MCLCCD_TUNE_WALK_BUFFER 11
+#define MCLCCD_TUNE_COUNT 12
 int mclccd_set_tuning(mclccd_tree *tree, int key, int value);
 int mclccd_get_tuning(const mclccd_tree *tree, int key, int *value);
 

@@ -86,6 +86,7 @@ def lib():
         "mclccd_set_tuning": ([vp, C.c_int, C.c_int], C.c_int),
         "mclccd_get_tuning": ([vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mclccd_kernel_launches": ([vp, llp], C.c_int),
+        "mclccd_build_stats": ([vp, llp, llp], C.c_int),
         "mclccd_last_error": ([vp], C.c_char_p),
         "mclccd_status_string": ([C.c_int], C.c_char_p),
     }
@@ -231,11 +232,12 @@ class BVHTree:
         self.precision = precision
 
     TUNE_KEYS = {"expand_grid": 0, "accd_grid": 1, "walk_packet": 2, "accd_rebin": 3, "walk_window": 4, "overlap": 5,
-                 "narrow_fused": 6, "fused_grid": 7, "walk_refill": 8}
+                 "narrow_fused": 6, "fused_grid": 7, "walk_refill": 8, "expand_split": 9,
+                 "rebuild_ratio": 10, "walk_buffer": 11}
 
     def set_tuning(self, **kv):
         """Launch-shape knobs (expand_grid, accd_grid, walk_packet, accd_rebin, walk_window, overlap,
-        narrow_fused, fused_grid, walk_refill); results never depend on them."""
+        narrow_fused, fused_grid, walk_refill, expand_split, rebuild_ratio, walk_buffer); results never depend on them."""
         for k, v in kv.items():
             self._check(self._L.mclccd_set_tuning(self._h, self.TUNE_KEYS[k], int(v)), self._h)
 
@@ -434,6 +436,12 @@ class BVHTree:
         n = C.c_longlong()
         self._L.mclccd_kernel_launches(self._h, C.byref(n))
         return n.value
+
+    def build_stats(self):
+        """(full hierarchy builds, of which caused by the tree-quality trigger)."""
+        b, q = C.c_longlong(), C.c_longlong()
+        self._check(self._L.mclccd_build_stats(self._h, C.byref(b), C.byref(q)), self._h)
+        return b.value, q.value
 
 
 def narrow_phase_bulk(V0, V1, sten, is_vf, vf_eta, ee_eta=None, stream: int | None = None,

@@ -142,11 +142,14 @@ __device__ void eval(const Stencil<DIM, VF> &S, double t, double &d, double (&w)
     for (int k = 0; k < DIM; ++k) { n[k] = sep[k] * inv; ft += n[k] * vel[k]; }
 }
 
-// Contact root and Jacobian row for one stencil: row[0..ns*DIM) = dt*/dV0,
-// row[ns*DIM..2 ns*DIM) = dt*/dV1 (slot-major).  Returns the status.
+// Contact root and the factors of the Jacobian row for one stencil: on kOk,
+// dt*/dV0 of slot i, coordinate k = c0 (w_i n_k) and dt*/dV1 = c1 (w_i n_k)
+// (jacobian_entry); otherwise the row is zero.  Returns the status.  The row
+// itself is formed by the caller, so its 2 (DIM + 1) DIM values are never
+// live during the root search.
 template <int DIM, bool VF>
 __device__ int toi_gradient(const double (&v0)[DIM + 1][DIM], const double (&v1)[DIM + 1][DIM], double eta,
-                            double toi, double &tstar, double (&row)[2 * (DIM + 1) * DIM])
+                            double toi, double &tstar, double (&w)[DIM + 1], double (&n)[DIM], double &c0, double &c1)
 {
     constexpr int ns = DIM + 1;
     Stencil<DIM, VF> S;
@@ -171,13 +174,12 @@ __device__ int toi_gradient(const double (&v0)[DIM + 1][DIM], const double (&v1)
             lmax = fmax(lmax, q);
         }
     const double l = sqrt(lmax) * (1.0 + 1e-12);
-#pragma unroll
-    for (int j = 0; j < 2 * ns * DIM; ++j) row[j] = 0.0;
+    c0 = c1 = 0.0;
     tstar = toi;
     if (toi == 0.0) return kToiZero;
     if (!(toi > 0.0) || !(toi <= 1.0) || !(l > 0.0) || !isfinite(l)) return kBadToi;
 
-    double w[ns], n[DIM], d, ft;
+    double d, ft;
     double t = toi;
     eval<DIM, VF>(S, t, d, w, n, ft);
     double f = d - eta;
@@ -223,15 +225,8 @@ __device__ int toi_gradient(const double (&v0)[DIM + 1][DIM], const double (&v1)
     tstar = t;
     if (!converged) return kNoConverge;
     if (!(ft < -1e-12 * l)) return kGrazing;   // not a transversal crossing
-    const double c0 = -(1.0 - t) / ft, c1 = -t / ft;
-#pragma unroll
-    for (int i = 0; i < ns; ++i)
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) {
-            const double gx = w[i] * n[k];
-            row[i * DIM + k] = c0 * gx;
-            row[ns * DIM + i * DIM + k] = c1 * gx;
-        }
+    c0 = -(1.0 - t) / ft;
+    c1 = -t / ft;
     return kOk;
 }
 
@@ -255,7 +250,7 @@ __device__ __forceinline__ bool gather_a(const int *s, const double *__restrict_
 
 // One thread per hit: row, t*, status, and g * row scattered into dV0 / dV1.
 template <int DIM>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
 k_vjp_toi(const int *__restrict__ sten, const unsigned char *__restrict__ is_vf, const double *__restrict__ toi,
           const double *__restrict__ g, long long n, const double *__restrict__ V0, const double *__restrict__ V1,
           int nv, double vf_eta, double ee_eta, double *__restrict__ dV0, double *__restrict__ dV1,
@@ -266,32 +261,41 @@ k_vjp_toi(const int *__restrict__ sten, const unsigned char *__restrict__ is_vf,
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += stride) {
         const int s[4] = {sten[4 * h], sten[4 * h + 1], sten[4 * h + 2], sten[4 * h + 3]};
-        double x0[ns][DIM], x1[ns][DIM], row[2 * ns * DIM], ts = toi[h];
+        double w[ns], nn[DIM], c0 = 0.0, c1 = 0.0, ts = toi[h];
         int st;
-        if (!gather_a<DIM>(s, V0, V1, nv, x0, x1)) {
-            st = kBadIndex;
-#pragma unroll
-            for (int j = 0; j < 2 * ns * DIM; ++j) row[j] = 0.0;
-        } else if (DIM == 3 && !is_vf[h]) {
-            st = toi_gradient<DIM, false>(x0, x1, ee_eta, toi[h], ts, row);
-        } else {
-            st = toi_gradient<DIM, true>(x0, x1, vf_eta, toi[h], ts, row);
+        {
+            double x0[ns][DIM], x1[ns][DIM];
+            if (!gather_a<DIM>(s, V0, V1, nv, x0, x1)) st = kBadIndex;
+            else if (DIM == 3 && !is_vf[h]) st = toi_gradient<DIM, false>(x0, x1, ee_eta, toi[h], ts, w, nn, c0, c1);
+            else st = toi_gradient<DIM, true>(x0, x1, vf_eta, toi[h], ts, w, nn, c0, c1);
         }
         if (t_star) t_star[h] = ts;
         if (status) status[h] = st;
+        const bool ok = st == kOk;
+        // row entries: c (w_i n_k), zero unless ok
         if (rows)
 #pragma unroll
-            for (int j = 0; j < 2 * ns * DIM; ++j) rows[h * 2 * ns * DIM + j] = row[j];
-        if (st == kOk) {
-            if (n_ok) atomicAdd(n_ok, 1ull);
+            for (int i = 0; i < ns; ++i)
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) {
+                    const double gx = ok ? w[i] * nn[k] : 0.0;
+                    rows[h * 2 * ns * DIM + i * DIM + k] = ok ? c0 * gx : 0.0;
+                    rows[h * 2 * ns * DIM + ns * DIM + i * DIM + k] = ok ? c1 * gx : 0.0;
+                }
+        if (ok) {
+            if (n_ok) {   // one atomic per warp
+                const unsigned m = __activemask();
+                if ((int)lane_id() == __ffs(m) - 1) atomicAdd(n_ok, (unsigned long long)__popc(m));
+            }
             const double gh = g ? g[h] : 0.0;
             if (gh != 0.0 && dV0 && dV1)
 #pragma unroll
                 for (int i = 0; i < ns; ++i)
 #pragma unroll
                     for (int k = 0; k < DIM; ++k) {
-                        atomicAdd(dV0 + (size_t)s[i] * DIM + k, gh * row[i * DIM + k]);
-                        atomicAdd(dV1 + (size_t)s[i] * DIM + k, gh * row[ns * DIM + i * DIM + k]);
+                        const double gx = w[i] * nn[k];
+                        atomicAdd(dV0 + (size_t)s[i] * DIM + k, gh * (c0 * gx));
+                        atomicAdd(dV1 + (size_t)s[i] * DIM + k, gh * (c1 * gx));
                     }
         }
     }

@@ -133,6 +133,17 @@ __global__ void k_karras(const unsigned *__restrict__ keys, int n, Node *__restr
 // climbs: the second thread to reach an internal node merges both child slots
 // and moves up (first arrival stops).  `visits` must be zero on entry.
 // ---------------------------------------------------------------------------
+// Surface area (3D; half of it) or perimeter (2D; half of it) of a swept box.
+template <int DIM>
+__device__ __forceinline__ float swept_area(const Box2T<DIM> &b)
+{
+    float e[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) e[c] = fmaxf(b.t0hi[c], b.t1hi[c]) - fminf(b.t0lo[c], b.t1lo[c]);
+    if constexpr (DIM == 3) return e[0] * e[1] + e[1] * e[2] + e[2] * e[0];
+    else return e[0] + e[1];
+}
+
 template <int DIM>
 __global__ void k_refit(const double *__restrict__ V0, const double *__restrict__ V1, const int *__restrict__ P,
                         int np, int pdim, int nv, double eta, const int *__restrict__ active,
@@ -292,6 +303,52 @@ void launch_refit(int dim, const double *V0, const double *V1, const int *P, int
     else
         k_refit<2><<<g, 256, 0, st>>>(V0, V1, P, np, pdim, nv, eta, active, sorted, leaf_parent, nodes, visits,
                                       reinterpret_cast<LeafBox<2> *>(leaf_box), leaf_active, cnt);
+}
+
+// Tree quality after a refit: over every node record (both children's
+// boxes), the summed areas of the internal children and of the leaf
+// children; coalesced reads of the node array, one atomic per block.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_tree_quality(const Node *__restrict__ nodes, int n_nodes, double *out)
+{
+    constexpr int S = DIM == 3 ? 3 : 2;
+    double inner = 0.0, leaves = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes; i += gridDim.x * blockDim.x) {
+        float4 ls[S], rs[S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) { ls[j] = __ldg(&nodes[i].l[j]); rs[j] = __ldg(&nodes[i].r[j]); }
+        const int meta = __ldg(&nodes[i].d.y);
+        Box2T<DIM> lb, rb;
+        unpack_child<DIM>(ls, lb);
+        unpack_child<DIM>(rs, rb);
+        const double al = swept_area<DIM>(lb), ar = swept_area<DIM>(rb);
+        if (meta & kMetaLeftLeaf) leaves += al; else inner += al;
+        if (meta & kMetaRightLeaf) leaves += ar; else inner += ar;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        inner += __shfl_xor_sync(0xffffffffu, inner, o);
+        leaves += __shfl_xor_sync(0xffffffffu, leaves, o);
+    }
+    __shared__ double s[2][8];
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 0) { s[0][w] = inner; s[1][w] = leaves; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += s[0][k]; b += s[1][k]; }
+        atomicAdd(out, a);
+        atomicAdd(out + 1, b);
+    }
+}
+
+void launch_tree_quality(int dim, const Node *nodes, int np, double *out, cudaStream_t st)
+{
+    cudaMemsetAsync(out, 0, 2 * sizeof(double), st);
+    if (np < 2) return;
+    const int g = grid_for(np - 1, 256, 148 * 8);
+    if (dim == 3) k_tree_quality<3><<<g, 256, 0, st>>>(nodes, np - 1, out);
+    else k_tree_quality<2><<<g, 256, 0, st>>>(nodes, np - 1, out);
 }
 
 void launch_owner_flags(const int *P, int np, int pdim, int nv, int *vowner, unsigned long long *ekeys, int *eowner,

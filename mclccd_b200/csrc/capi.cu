@@ -68,12 +68,18 @@ struct mclccd_tree {
     DevBuf in_V, in_P, in_act, in_tmp;   // input conversion staging (mclccd_update_ex / mclccd_traverse_ex)
     DevBuf cand_cnt;                     // counters of the on-request candidate expansion
     DevBuf walk_cursor;                  // query cursor of the refill walk
+    DevBuf quality;                      // summed box areas of the internal nodes and of the leaves
+    double *h_quality = nullptr;         // pinned copy of the two sums
+    double q_build = 0.0;                // tree quality (internal / leaf box areas) after the last build
+    bool force_rebuild = false;          // the refit-only tree degraded: rebuild at the next update
+    long long n_builds = 0, n_quality_rebuilds = 0;
+    DevBuf tq_idx, tq_state, tq_count;   // continuing-stencil queue of the split ACCD form
     std::vector<DevBuf *> all()
     {
         return {&V0d, &V1d, &Pd, &Pstage, &actd, &pflags, &pflags_tmp, &vowner, &ekeys, &eowner, &cent, &bounds,
                 &keys, &vals, &keys_alt, &vals_alt, &sort_scratch, &nodes, &leaf_parent, &visits, &leaf_box,
                 &leaf_active, &pairs, &vf, &ee, &hit_sten, &hit_toi, &hit_isvf, &disc, &counters, &diff,
-                &fp64_queue, &in_V, &in_P, &in_act, &in_tmp, &cand_cnt, &walk_cursor};
+                &fp64_queue, &in_V, &in_P, &in_act, &in_tmp, &cand_cnt, &walk_cursor, &tq_idx, &tq_state, &tq_count, &quality};
     }
     Counters *h_cnt = nullptr;   // pinned mirror of the device counters
     int *h_diff = nullptr;
@@ -89,7 +95,7 @@ struct mclccd_tree {
     cudaEvent_t out_ev[16] = {};
     unsigned long long *h_snap = nullptr;
     unsigned long long out_done = 0;   // hits already copied out by the streamed path
-    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0, 0, kFusedGrid, 0};
+    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0, 0, kFusedGrid, 0, 0, 150, 0};
     // The fused narrow phase counts the candidate lists without writing them;
     // mclccd_get_candidates rebuilds them from the leaf pairs and the P of the
     // last traverse.
@@ -166,10 +172,37 @@ static int launch_walk(mclccd_tree *t, int dim, int packet, int np, Counters *cn
                                np, as<int2>(t->pairs), t->cap_pairs, cnt, as<unsigned>(t->walk_cursor), st, qb, qe);
         return MCLCCD_OK;
     }
+    if (!packet && t->tune[MCLCCD_TUNE_WALK_BUFFER]) {
+        launch_traverse_buffered(dim, t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes), t->leaf_box.p,
+                                 as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs),
+                                 t->cap_pairs, cnt, st, qb, qe);
+        return MCLCCD_OK;
+    }
     launch_traverse(dim, packet, t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes), t->leaf_box.p,
                     as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs), t->cap_pairs, cnt, st,
                     qb, qe);
     return MCLCCD_OK;
+}
+
+// Leaf pairs [*lo, *hi) -> stencil lists and discrete pairs: one kernel, or
+// (MCLCCD_TUNE_EXPAND_SPLIT) the stencil expansion and the discrete test as
+// two kernels.  Returns the launches made.
+static int launch_expand(mclccd_tree *t, int dim, const int *dP, const double *dV1, int nv, int cont, bool discr,
+                         Counters *cnt, cudaStream_t st, const unsigned long long *lo = nullptr,
+                         const unsigned long long *hi = nullptr)
+{
+    if (t->tune[MCLCCD_TUNE_EXPAND_SPLIT] && discr && cont) {
+        launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                            as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
+                            cont, 0, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st, lo, hi);
+        launch_discrete_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, dV1, nv, as<int2>(t->disc), t->cap_disc, cnt,
+                              148 * 16, st, lo, hi);
+        return 2;
+    }
+    launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
+                        as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc, cont,
+                        discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st, lo, hi);
+    return 1;
 }
 
 // Inputs in other forms than row-major double (float coordinates, column-
@@ -291,9 +324,7 @@ static int enqueue_overlapped(mclccd_tree *t, int chunks, int dim, int np, int n
                                 t->tune[MCLCCD_TUNE_FUSED_GRID], t->s_narrow, pe + c, pe + c + 1);
             t->launches += 2;
         } else {
-            launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
-                                as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
-                                1, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], t->s_narrow, pe + c, pe + c + 1);
+            t->launches += launch_expand(t, dim, dP, dV1, nv, 1, discr, cnt, t->s_narrow, pe + c, pe + c + 1) - 1;
             launch_snapshot(&cnt->n_vf, ve + c + 1, &cnt->n_ee, ee + c + 1, t->s_narrow);
             accd(true, t->vf, ve + c + 1, t->cap_vf, t->vf_eta, ve + c, t->s_narrow);
             if (dim == 3) accd(false, t->ee, ee + c + 1, t->cap_ee, t->ee_eta, ee + c, t->s_narrow);
@@ -355,9 +386,7 @@ static int enqueue_streamed(mclccd_tree *t, int dim, int np, int nv, const int *
                                 t->tune[MCLCCD_TUNE_FUSED_GRID], st, pe + c, pe + c + 1);
             t->launches += 3;
         } else {
-            launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
-                                as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
-                                1, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st, pe + c, pe + c + 1);
+            t->launches += launch_expand(t, dim, dP, dV1, nv, 1, discr, cnt, st, pe + c, pe + c + 1) - 1;
             launch_snapshot(&cnt->n_vf, ve + c + 1, &cnt->n_ee, ee + c + 1, st);
             accd(true, t->vf, ve + c + 1, t->cap_vf, t->vf_eta, ve + c, st);
             if (dim == 3) accd(false, t->ee, ee + c + 1, t->cap_ee, t->ee_eta, ee + c, st);
@@ -449,6 +478,7 @@ int mclccd_create(int dim, mclccd_tree **out)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&t->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&t->h_cnt, sizeof(Counters));
     if (e == cudaSuccess) e = cudaMallocHost(&t->h_diff, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&t->h_quality, 2 * sizeof(double));
     for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&t->ev[i]);
     if (e == cudaSuccess) e = ensure(t->counters, sizeof(Counters));
     if (e == cudaSuccess) e = ensure(t->diff, 2 * sizeof(int));
@@ -481,6 +511,7 @@ int mclccd_destroy(mclccd_tree *t)
     if (t->ovl.p) cudaFree(t->ovl.p);
     if (t->h_cnt) cudaFreeHost(t->h_cnt);
     if (t->h_diff) cudaFreeHost(t->h_diff);
+    if (t->h_quality) cudaFreeHost(t->h_quality);
     if (t->own_stream) cudaStreamDestroy(t->own_stream);
     delete t;
     return MCLCCD_OK;
@@ -554,7 +585,7 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
     MC_CUDA(t, ensure(t->Pstage, sizeof(int) * (size_t)pcount));
     // Refit-only when the topology is byte-identical to the previous update.
     const bool may_refit = t->built && t->np > 1 && !(t->flags & MCLCCD_OPT_ALWAYS_REBUILD) && np == t->np &&
-                           pdim == t->pdim;
+                           pdim == t->pdim && !t->force_rebuild;
     int p_known = -1;   // -1: P not compared yet; 0 / 1: P differs / equals the stored P
     const bool derive_nv = nv == 0;
     if (derive_nv) {
@@ -658,13 +689,38 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
     MC_CUDA(t, ensure(t->leaf_box, sizeof(double) * 4 * dim * (size_t)np));
     MC_CUDA(t, ensure(t->leaf_active, (size_t)np));
     MC_CUDA(t, ensure(t->visits, sizeof(int) * (size_t)std::max(1, np - 1)));
+    // tree quality: the refit also sums the box areas of its internal nodes
+    // and of its leaves
+    const bool track = np > 1 && t->tune[MCLCCD_TUNE_REBUILD_RATIO] > 0;
     launch_refit(dim, dV0, dV1, dP, np, pdim, nv, t->box_eta, dact, as<int>(t->vals), as<int>(t->leaf_parent),
                  as<Node>(t->nodes), as<int>(t->visits), t->leaf_box.p, as<unsigned char>(t->leaf_active), cnt, st);
     ++t->launches;
+    if (track) {
+        MC_CUDA(t, ensure(t->quality, 2 * sizeof(double)));
+        launch_tree_quality(dim, as<Node>(t->nodes), np, as<double>(t->quality), st);
+        ++t->launches;
+    }
     if (int rc = check_launch(t, "refit kernel")) return rc;
     if (prof) cudaEventRecord(t->ev[2], st);
     MC_CUDA(t, cudaMemcpyAsync(t->h_cnt, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    if (track)
+        MC_CUDA(t, cudaMemcpyAsync(t->h_quality, t->quality.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
     MC_CUDA(t, cudaStreamSynchronize(st));
+    if (!same) ++t->n_builds;
+    if (t->force_rebuild && !same) ++t->n_quality_rebuilds;
+    t->force_rebuild = false;
+    if (track) {
+        // quality = internal-node box areas / leaf box areas (the surface-area
+        // cost of the hierarchy, normalised by the geometry's own).  A
+        // refit-only tree whose quality grew past the ratio of the last
+        // build's is rebuilt at the next update: the Morton order of the
+        // positions it was built from no longer fits the motion.
+        const double inner = t->h_quality[0], leaves = t->h_quality[1];
+        const double q = leaves > 0.0 ? inner / leaves : 0.0;
+        if (!same) t->q_build = q;
+        else if (t->q_build > 0.0 && q > t->q_build * (t->tune[MCLCCD_TUNE_REBUILD_RATIO] / 100.0))
+            t->force_rebuild = true;
+    }
     if (prof) {
         cudaEventElapsedTime(&t->stage[0], t->ev[0], t->ev[2]);
         cudaEventElapsedTime(&t->stage[1], t->ev[0], t->ev[1]);
@@ -849,6 +905,12 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
         MC_CUDA(t, ensure(t->hit_toi, sizeof(double) * t->cap_hits));
         MC_CUDA(t, ensure(t->hit_isvf, t->cap_hits));
         MC_CUDA(t, ensure(t->disc, sizeof(int2) * t->cap_disc));
+        if (cont && !fused && !certified && t->tune[MCLCCD_TUNE_ACCD_REBIN] == 2) {
+            const size_t qn = std::max(t->cap_vf, t->cap_ee);
+            MC_CUDA(t, ensure(t->tq_idx, sizeof(unsigned) * qn));
+            MC_CUDA(t, ensure(t->tq_state, sizeof(double2) * qn));
+            MC_CUDA(t, ensure(t->tq_count, sizeof(unsigned long long)));
+        }
         if (certified && cont) MC_CUDA(t, ensure(t->fp64_queue, sizeof(unsigned) * std::max(t->cap_vf, t->cap_ee)));
         MC_CUDA(t, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
         // narrow phase of one list, stencils [*lo, *n) (lo == nullptr: from 0)
@@ -864,10 +926,16 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
                                       as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits,
                                       as<unsigned>(t->fp64_queue), cnt, t->tune[MCLCCD_TUNE_ACCD_GRID], s);
                 t->launches += 2;
+            } else if (t->tune[MCLCCD_TUNE_ACCD_REBIN] == 2) {   // head and tail kernels over a queue
+                launch_accd_split(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
+                                  as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
+                                  t->tune[MCLCCD_TUNE_ACCD_GRID], as<unsigned>(t->tq_idx), as<double2>(t->tq_state),
+                                  as<unsigned long long>(t->tq_count), s, lo);
+                t->launches += 2;
             } else {
                 launch_accd_pipeline(dim, vf, as<int4>(list), n_ptr, cap, dV0, dV1, nv, eta, as<int4>(t->hit_sten),
                                      as<double>(t->hit_toi), as<unsigned char>(t->hit_isvf), t->cap_hits, cnt,
-                                     t->tune[MCLCCD_TUNE_ACCD_GRID], t->tune[MCLCCD_TUNE_ACCD_REBIN] != 0, s, lo);
+                                     t->tune[MCLCCD_TUNE_ACCD_GRID], t->tune[MCLCCD_TUNE_ACCD_REBIN] == 1, s, lo);
                 ++t->launches;
             }
         };
@@ -890,9 +958,7 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
                                     t->cap_hits, cnt, t->tune[MCLCCD_TUNE_FUSED_GRID], st);
                 t->launches += 2;
             } else {
-                launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
-                                    as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc),
-                                    t->cap_disc, cont, discr, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st);
+                t->launches += launch_expand(t, dim, dP, dV1, nv, cont, discr, cnt, st) - 1;
                 if (prof) cudaEventRecord(t->ev[5], st);
                 t->launches += 2;
                 if (cont) {
@@ -1344,6 +1410,14 @@ int mclccd_get_tree_host(mclccd_tree *t, void *nodes, double *leaf_box, int *lea
     return MCLCCD_OK;
 }
 
+int mclccd_build_stats(const mclccd_tree *t, long long *builds, long long *quality_rebuilds)
+{
+    if (!t) return MCLCCD_ERR_INVALID;
+    if (builds) *builds = t->n_builds;
+    if (quality_rebuilds) *quality_rebuilds = t->n_quality_rebuilds;
+    return MCLCCD_OK;
+}
+
 int mclccd_tree_size(const mclccd_tree *t, int *nv, int *np, int *pdim)
 {
     if (!t) return MCLCCD_ERR_INVALID;
@@ -1388,18 +1462,24 @@ int mclccd_stage_ms(const mclccd_tree *t, float *ms, int n)
 int mclccd_set_tuning(mclccd_tree *t, int key, int value)
 {
     if (!t || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
-    const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_ACCD_REBIN ||
-                      key == MCLCCD_TUNE_NARROW_FUSED || key == MCLCCD_TUNE_WALK_REFILL;
-    if (key == MCLCCD_TUNE_OVERLAP) {
+    const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_NARROW_FUSED ||
+                      key == MCLCCD_TUNE_WALK_REFILL || key == MCLCCD_TUNE_EXPAND_SPLIT ||
+                      key == MCLCCD_TUNE_WALK_BUFFER;
+    if (key == MCLCCD_TUNE_REBUILD_RATIO) {
+        if (value != 0 && (value < 101 || value > 100000))
+            return fail(t, MCLCCD_ERR_INVALID, "rebuild ratio is 0 (never) or a percentage above 100");
+    } else if (key == MCLCCD_TUNE_ACCD_REBIN) {
+        if (value < 0 || value > 2) return fail(t, MCLCCD_ERR_INVALID, "ACCD form must be 0, 1 or 2");
+    } else if (key == MCLCCD_TUNE_OVERLAP) {
         if (value < 0 || value > 16) return fail(t, MCLCCD_ERR_INVALID, "overlap chunks must be in [0, 16]");
     } else if (key == MCLCCD_TUNE_WALK_WINDOW) {
         if (value != 0 && value != 8 && value != 16 && value != 32 && value != 64 && value != 128)
             return fail(t, MCLCCD_ERR_INVALID, "walk window must be 0, 8, 16, 32, 64 or 128");
-        if (t->tune[MCLCCD_TUNE_WALK_REFILL] && (value == 0 || value > 32))
-            return fail(t, MCLCCD_ERR_INVALID, "the refill walk takes a window of 8, 16 or 32");
-    } else if (key == MCLCCD_TUNE_WALK_REFILL && value == 1 &&
+        if ((t->tune[MCLCCD_TUNE_WALK_REFILL] || t->tune[MCLCCD_TUNE_WALK_BUFFER]) && (value == 0 || value > 32))
+            return fail(t, MCLCCD_ERR_INVALID, "the refill and buffered walks take a window of 8, 16 or 32");
+    } else if ((key == MCLCCD_TUNE_WALK_REFILL || key == MCLCCD_TUNE_WALK_BUFFER) && value == 1 &&
                (t->tune[MCLCCD_TUNE_WALK_WINDOW] == 0 || t->tune[MCLCCD_TUNE_WALK_WINDOW] > 32)) {
-        return fail(t, MCLCCD_ERR_INVALID, "the refill walk takes a window of 8, 16 or 32");
+        return fail(t, MCLCCD_ERR_INVALID, "the refill and buffered walks take a window of 8, 16 or 32");
     } else if (flag ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))
         return fail(t, MCLCCD_ERR_INVALID, "tuning value out of range");
     t->tune[key] = value;

@@ -158,6 +158,50 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *c
     return base + (incl - k);
 }
 
+// Block-wide (every thread of the block must call, blockDim.x == BLOCK)
+// reservation of a slots on counter ca and b slots on counter cb per thread:
+// one atomic per counter per block instead of one per warp, so a kernel whose
+// warps all append to the same list does not queue on that counter in L2.
+// a, b < 2^16 per thread and their block totals < 2^16.  Returns the
+// thread's first slot on each counter.
+template <int BLOCK>
+__device__ __forceinline__ void block_reserve2(unsigned long long *ca, unsigned a, unsigned long long *cb, unsigned b,
+                                               unsigned long long &sa, unsigned long long &sb)
+{
+    constexpr int W = BLOCK / 32;
+    __shared__ unsigned s_warp[W];
+    __shared__ unsigned long long s_base[2];
+    const unsigned k = a | (b << 16);
+    unsigned incl = k;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)lane_id() >= o) incl += v;
+    }
+    const int warp = threadIdx.x >> 5;
+    if (lane_id() == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned tot = lane_id() < W ? s_warp[lane_id()] : 0u;
+        unsigned sc = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned v = __shfl_up_sync(0xffffffffu, sc, o);
+            if ((int)lane_id() >= o) sc += v;
+        }
+        if (lane_id() < W) s_warp[lane_id()] = sc - tot;   // exclusive offsets of the warps
+        if (lane_id() == 31) {
+            s_base[0] = (sc & 0xffffu) ? atomicAdd(ca, (unsigned long long)(sc & 0xffffu)) : 0ull;
+            s_base[1] = (sc >> 16) ? atomicAdd(cb, (unsigned long long)(sc >> 16)) : 0ull;
+        }
+    }
+    __syncthreads();
+    const unsigned off = s_warp[warp] + (incl - k);
+    sa = s_base[0] + (off & 0xffffu);
+    sb = s_base[1] + (off >> 16);
+    __syncthreads();   // the next call may overwrite s_warp / s_base
+}
+
 // Monotone float <-> uint mapping for atomic min/max of floats.
 __device__ __forceinline__ unsigned float_to_ordered(float f)
 {

@@ -14,6 +14,9 @@ void launch_karras(const unsigned *keys, int n, Node *nodes, int *leaf_parent, c
 void launch_refit(int dim, const double *V0, const double *V1, const int *P, int np, int pdim, int nv, double eta,
                   const int *active, const int *sorted, const int *leaf_parent, Node *nodes, int *visits,
                   void *leaf_box, unsigned char *leaf_active, Counters *cnt, cudaStream_t st);
+// out[0] = summed surface areas (perimeters in 2D) of the internal nodes'
+// swept boxes, out[1] = of the leaves' boxes (2 device doubles)
+void launch_tree_quality(int dim, const Node *nodes, int np, double *out, cudaStream_t st);
 void launch_owner_flags(const int *P, int np, int pdim, int nv, int *vowner, unsigned long long *ekeys, int *eowner,
                         unsigned long long ecap, unsigned char *flags, Counters *cnt, cudaStream_t st);
 void launch_compare(const int *a, const int *b, long long n, int *diff, cudaStream_t st);
@@ -41,6 +44,15 @@ void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap
                          int4 *ee, unsigned long long ee_cap, int2 *disc, unsigned long long disc_cap, int continuous,
                          int discrete, Counters *cnt, int grid, cudaStream_t st,
                          const unsigned long long *lo_ptr = nullptr, const unsigned long long *hi_ptr = nullptr);
+// the discrete test of leaf pairs [*lo, *hi) alone (hi == nullptr: the pair count)
+// the window walk with pairs collected per warp and written 32 at a time
+void launch_traverse_buffered(int dim, int window, const Node *nodes, const void *leaf_box,
+                              const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs,
+                              unsigned long long cap, Counters *cnt, cudaStream_t st, int q_begin = 0,
+                              int q_end = -1);
+void launch_discrete_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P, const double *V1,
+                           int nv, int2 *disc, unsigned long long disc_cap, Counters *cnt, int grid, cudaStream_t st,
+                           const unsigned long long *lo_ptr = nullptr, const unsigned long long *hi_ptr = nullptr);
 void launch_snapshot(const unsigned long long *a, unsigned long long *da, const unsigned long long *b,
                      unsigned long long *db, cudaStream_t st);
 
@@ -49,6 +61,13 @@ void launch_accd_pipeline(int dim, bool vf, const int4 *sten, const unsigned lon
                           const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
                           unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, bool rebin,
                           cudaStream_t st, const unsigned long long *lo_ptr = nullptr);
+// narrow.cu: the head / tail split of the FP64 ACCD over one list (two
+// launches; q_idx / q_state hold up to cap entries, q_count is zeroed here)
+void launch_accd_split(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
+                       const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
+                       unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, unsigned *q_idx,
+                       double2 *q_state, unsigned long long *q_count, cudaStream_t st,
+                       const unsigned long long *lo_ptr = nullptr);
 // fused.cu: leaf pairs [*lo, *hi) -> stencils -> discrete test + FP64 ACCD in
 // one kernel (candidate lists counted, not written)
 void launch_narrow_fused(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P,

@@ -30,6 +30,43 @@ __device__ __forceinline__ bool gather_stencil(const int *s, const double *__res
     return ok;
 }
 
+// The reference loop as written, out of line with its own gathers, for the
+// rare stencil whose iteration 0 is not an exact no-op (non-finite or -0.0
+// coordinates): the callers' arrays stay in registers.  -1 on a miss.
+template <int DIM, bool VF>
+__device__ __noinline__ double literal_regather(int4 s4, const double *__restrict__ V0, const double *__restrict__ V1,
+                                                int nv, double eta, Counters *cnt)
+{
+    const int s[4] = {s4.x, s4.y, s4.z, s4.w};
+    double v0[DIM + 1][DIM], v1[DIM + 1][DIM], toi = -1.0;
+    int iters;
+    gather_stencil<DIM>(s, V0, V1, nv, v0, v1);
+    const int hit = accd_literal<DIM, VF>(v0, v1, eta, toi, iters);
+    if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
+    return hit ? toi : -1.0;
+}
+
+// ACCD of one gathered stencil with the literal path out of line; toi = -1
+// on a miss, otherwise the reference's toi.
+template <int DIM, bool VF>
+__device__ __forceinline__ double accd_stencil(const int4 &s4, const double (&v0)[DIM + 1][DIM],
+                                               const double (&v1)[DIM + 1][DIM], const double *__restrict__ V0,
+                                               const double *__restrict__ V1, int nv, double eta, Counters *cnt)
+{
+    double p[DIM + 1][DIM], x[DIM + 1][DIM], l_p, d0, t_l1;
+    bool noop;
+    accd_setup<DIM, VF, true>(v0, v1, p, x, l_p, noop);
+    const int h = accd_head_fast<DIM, VF>(x, l_p, noop, eta, d0, t_l1);
+    if (h == kHeadHit) return 0.0;
+    if (h == kHeadMiss) return -1.0;
+    if (h == kHeadLiteral) return literal_regather<DIM, VF>(s4, V0, V1, nv, eta, cnt);
+    double toi = -1.0;
+    int iters;
+    const int hit = accd_resume<DIM, VF>(x, p, l_p, eta, d0, toi, iters);
+    if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
+    return hit ? toi : -1.0;
+}
+
 // Resident 128-thread blocks per SM the pipeline ACCD kernel is compiled for
 // (register cap = 64K / (128 x this)); the kernel is latency-bound, so more
 // resident warps beat a few spilled registers.
@@ -55,13 +92,11 @@ k_accd_pipeline(const int4 *__restrict__ sten, const unsigned long long *n_ptr, 
         const int s[4] = {s4.x, s4.y, s4.z, s4.w};
         double x0[DIM + 1][DIM], x1[DIM + 1][DIM];
         if (!gather_stencil<DIM>(s, V0, V1, nv, x0, x1)) { atomicOr(&cnt->err, kErrBadIndex); continue; }
-        double toi = -1.0;
-        int iters;
-        const int hit = accd<DIM, VF>(x0, x1, eta, toi, iters);
-        if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
+        const double toi = accd_stencil<DIM, VF>(s4, x0, x1, V0, V1, nv, eta, cnt);
         // collide() delivers a hit only when toi >= 0 (BVHTree.cpp:262): a
-        // degenerate stencil can report hit == 1 with toi = NaN.
-        if (hit && toi >= 0.0) {
+        // degenerate stencil can report hit == 1 with toi = NaN, which the
+        // comparison rejects.
+        if (toi >= 0.0) {
             const unsigned long long slot = warp_append(&cnt->n_hits);
             if (slot < hit_cap) {
                 hit_sten[slot] = s4;
@@ -187,6 +222,118 @@ k_accd_rebin(const int4 *__restrict__ sten, const unsigned long long *n_ptr, uns
         const double t = tail(tid);
         rebin_emit<DIM, VF>(q_sten[tid], t, t >= 0.0, cnt, hit_sten, hit_toi, hit_isvf, hit_cap);
     }
+}
+
+// Split form (MCLCCD_TUNE_ACCD_REBIN = 2): the head of ACCD in one kernel
+// over the whole list, the tail in a second kernel over the stencils that go
+// on.  About 40% of a cloth's stencils are decided by their first distance
+// and the rest need two more, so in the one-kernel form the lanes of a warp
+// wait on each other; here every warp of the head kernel runs one distance
+// per lane and every warp of the tail kernel (almost always) two.  The head
+// appends (list index, d0, l_p) of each continuing stencil to a queue; the
+// tail re-gathers the stencil and its positions, rebuilds the motion exactly
+// (setup without the norms) and resumes the reference loop at iteration 1,
+// so (hit, toi) are bit-identical to the one-kernel form.
+template <int DIM, bool VF>
+__global__ void __launch_bounds__(128, MCLCCD_ACCD_MIN_BLOCKS)
+k_accd_head(const int4 *__restrict__ sten, const unsigned long long *n_ptr, unsigned long long cap,
+            const double *__restrict__ V0, const double *__restrict__ V1, int nv, double eta,
+            int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,
+            unsigned long long hit_cap, Counters *cnt, const unsigned long long *lo_ptr, unsigned *__restrict__ q_idx,
+            double2 *__restrict__ q_state, unsigned long long *q_count)
+{
+    unsigned long long n = *(volatile const unsigned long long *)n_ptr;
+    if (n > cap) n = cap;
+    const unsigned long long lo = lo_ptr ? min(*(volatile const unsigned long long *)lo_ptr, n) : 0ull;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int4 s4 = sten[i];
+        const int s[4] = {s4.x, s4.y, s4.z, s4.w};
+        double v0[DIM + 1][DIM], v1[DIM + 1][DIM];
+        if (!gather_stencil<DIM>(s, V0, V1, nv, v0, v1)) { atomicOr(&cnt->err, kErrBadIndex); continue; }
+        double p[DIM + 1][DIM], x[DIM + 1][DIM], l_p, d0 = 0.0, t_l1;
+        bool noop;
+        accd_setup<DIM, VF, true>(v0, v1, p, x, l_p, noop);
+        const int h = accd_head_fast<DIM, VF>(x, l_p, noop, eta, d0, t_l1);
+        double toi = -1.0;
+        bool hit = false;
+        if (h == kHeadHit) {
+            toi = 0.0;
+            hit = true;
+        } else if (h == kHeadLiteral) {   // iteration 0 is not an exact no-op: the reference loop as written
+            toi = literal_regather<DIM, VF>(s4, V0, V1, nv, eta, cnt);
+            hit = toi >= 0.0;
+        } else if (h == kHeadContinue) {
+            const unsigned long long slot = warp_append(q_count);   // < cap: one entry per stencil
+            q_idx[slot] = (unsigned)i;
+            q_state[slot] = make_double2(d0, l_p);
+        }
+        if (hit && toi >= 0.0) {   // collide() delivers a hit only when toi >= 0 (BVHTree.cpp:262)
+            const unsigned long long slot = warp_append(&cnt->n_hits);
+            if (slot < hit_cap) {
+                hit_sten[slot] = s4;
+                hit_toi[slot] = toi;
+                hit_isvf[slot] = VF ? 1 : 0;
+            }
+        }
+    }
+}
+
+#ifndef MCLCCD_ACCD_TAIL_MIN_BLOCKS
+#define MCLCCD_ACCD_TAIL_MIN_BLOCKS 6
+#endif
+template <int DIM, bool VF>
+__global__ void __launch_bounds__(128, MCLCCD_ACCD_TAIL_MIN_BLOCKS)
+k_accd_tail(const int4 *__restrict__ sten, const double *__restrict__ V0, const double *__restrict__ V1, int nv,
+            double eta, int4 *__restrict__ hit_sten, double *__restrict__ hit_toi, unsigned char *__restrict__ hit_isvf,
+            unsigned long long hit_cap, Counters *cnt, const unsigned *__restrict__ q_idx,
+            const double2 *__restrict__ q_state, const unsigned long long *q_count)
+{
+    const unsigned long long n = *(volatile const unsigned long long *)q_count;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const int4 s4 = sten[q_idx[j]];
+        const double2 st = q_state[j];
+        const int s[4] = {s4.x, s4.y, s4.z, s4.w};
+        double v0[DIM + 1][DIM], v1[DIM + 1][DIM], p[DIM + 1][DIM], x[DIM + 1][DIM], unused;
+        bool noop;
+        gather_stencil<DIM>(s, V0, V1, nv, v0, v1);   // indices checked by the head
+        accd_setup<DIM, VF, false>(v0, v1, p, x, unused, noop);
+        double toi = -1.0;
+        int iters;
+        const int hit = accd_resume<DIM, VF>(x, p, st.y, eta, st.x, toi, iters);
+        if (iters >= 1000) atomicOr(&cnt->err, kErrAccdIters);
+        if (hit && toi >= 0.0) {
+            const unsigned long long slot = warp_append(&cnt->n_hits);
+            if (slot < hit_cap) {
+                hit_sten[slot] = s4;
+                hit_toi[slot] = toi;
+                hit_isvf[slot] = VF ? 1 : 0;
+            }
+        }
+    }
+}
+
+void launch_accd_split(int dim, bool vf, const int4 *sten, const unsigned long long *n_ptr, unsigned long long cap,
+                       const double *V0, const double *V1, int nv, double eta, int4 *hit_sten, double *hit_toi,
+                       unsigned char *hit_isvf, unsigned long long hit_cap, Counters *cnt, int grid, unsigned *q_idx,
+                       double2 *q_state, unsigned long long *q_count, cudaStream_t st,
+                       const unsigned long long *lo_ptr)
+{
+    cudaMemsetAsync(q_count, 0, sizeof(unsigned long long), st);
+#define MCLCCD_SPLIT(D, K)                                                                                         \
+    {                                                                                                              \
+        k_accd_head<D, K><<<grid, 128, 0, st>>>(sten, n_ptr, cap, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf,    \
+                                                hit_cap, cnt, lo_ptr, q_idx, q_state, q_count);                    \
+        k_accd_tail<D, K><<<grid, 128, 0, st>>>(sten, V0, V1, nv, eta, hit_sten, hit_toi, hit_isvf, hit_cap, cnt,  \
+                                                q_idx, q_state, q_count);                                          \
+    }
+    if (dim == 3) {
+        if (vf) MCLCCD_SPLIT(3, true) else MCLCCD_SPLIT(3, false)
+    } else {
+        MCLCCD_SPLIT(2, true)
+    }
+#undef MCLCCD_SPLIT
 }
 
 // One-sided VF narrow phase (CTCD with the wrong-side test): 1 hit, 0 no

@@ -379,6 +379,139 @@ k_traverse_refill(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict
     }
 }
 
+// Buffered form of the window walk (MCLCCD_TUNE_WALK_BUFFER): the same tests
+// in the same order, with the pairs a warp finds collected in a per-warp
+// shared-memory buffer and written out 32 at a time with one atomic on the
+// pair counter, instead of one atomic per leaf test that hits.  The warp's
+// loops run in step (a lane that is done idles until the whole warp is), so
+// every flush is a whole-warp operation.
+template <int DIM, int W>
+__global__ void __launch_bounds__(128, 4)
+k_traverse_window_buf(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
+                      const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
+                      int q_begin, int q_end, int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
+{
+    constexpr int S = DIM == 3 ? 3 : 2;
+    constexpr int NB = 127 + W;
+    constexpr int OUT = 96;   // < 32 left after a flush + at most 64 per step
+    __shared__ float s_box[NB][4 * DIM];
+    __shared__ unsigned char s_act[NB];
+    __shared__ int stack[kStackDepth][128];
+    __shared__ int2 s_out[4][OUT];
+    __shared__ int s_nout[4];
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const unsigned full = 0xffffffffu;
+    const int q0 = q_begin + blockIdx.x * 128;
+    if (q0 >= q_end) return;   // whole block past the end
+    for (int i = tid; i < NB; i += 128) {
+        const int k = q0 + 1 + i;
+        if (k < n) {
+            const Box2T<DIM> kb = outward<DIM>(leaf_box[k]);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                s_box[i][d] = kb.t0lo[d];
+                s_box[i][DIM + d] = kb.t0hi[d];
+                s_box[i][2 * DIM + d] = kb.t1lo[d];
+                s_box[i][3 * DIM + d] = kb.t1hi[d];
+            }
+            s_act[i] = leaf_active[k];
+        }
+    }
+    if (lane == 0) s_nout[w] = 0;
+    __syncthreads();
+    const int q = q0 + tid;
+    const bool valid = q < q_end;
+    const int qq = valid ? q : q_end - 1;
+    const bool qact = leaf_active[qq] != 0;
+    const int qprim = sorted[qq];
+    const Box2T<DIM> qbox = outward<DIM>(leaf_box[qq]);
+
+    // whole warp: write out the buffered pairs, all of them or whole 32s
+    auto flush = [&](bool all) {
+        __syncwarp();
+        const int c = s_nout[w];
+        const int take = all ? c : (c & ~31);
+        if (take == 0) return;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&cnt->n_pairs, (unsigned long long)take);
+        base = __shfl_sync(full, base, 0);
+        for (int i = lane; i < take; i += 32)
+            if (base + i < cap) pairs[base + i] = s_out[w][i];
+        __syncwarp();
+        const int rest = c - take;   // < 32 <= take: source and destination do not overlap
+        if (lane < rest) s_out[w][lane] = s_out[w][take + lane];
+        __syncwarp();
+        if (lane == 0) s_nout[w] = rest;
+        __syncwarp();
+    };
+    auto leaf = [&](int k, const Box2T<DIM> &kbox) {
+        int r = leaf_test3<DIM>(qbox, inner<DIM>(qbox), kbox);
+        if (r == 2) r = leaf_boxes_intersect<DIM>(leaf_box[qq], leaf_box[k]) ? 1 : 0;
+        if (r == 1) {
+            const int kprim = __ldg(sorted + k);
+            const unsigned m = __activemask();
+            const int leader = __ffs(m) - 1;
+            int pos = 0;
+            if (lane == leader) pos = atomicAdd(&s_nout[w], __popc(m));
+            pos = __shfl_sync(m, pos, leader) + __popc(m & lanemask_lt());
+            s_out[w][pos] = make_int2(min(qprim, kprim), max(qprim, kprim));
+        }
+    };
+    // 1. the window: leaves q + 1 .. q + W from shared memory, in step
+    const int qw = min(qq + W, n - 1);
+    for (int j = 1; j <= W; ++j) {
+        flush(false);
+        const int k = qq + j;
+        if (!valid || k > qw) continue;
+        const int i = k - q0 - 1;
+        if (!(qact || s_act[i])) continue;
+        Box2T<DIM> kb;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            kb.t0lo[d] = s_box[i][d]; kb.t0hi[d] = s_box[i][DIM + d];
+            kb.t1lo[d] = s_box[i][2 * DIM + d]; kb.t1hi[d] = s_box[i][3 * DIM + d];
+        }
+        leaf(k, kb);
+    }
+    // 2. the tree beyond the window, one node per lane per step, in step
+    int sp = 0, node = 0, steps = 0;
+    bool done = !valid;
+    while (__any_sync(full, !done)) {
+        flush(false);
+        if (done) continue;
+        if (++steps > n) { atomicOr(&cnt->err, kErrStack); done = true; continue; }
+        float4 ls[S], rs[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) { ls[i] = __ldg(&nodes[node].l[i]); rs[i] = __ldg(&nodes[node].r[i]); }
+        const int4 d = __ldg(&nodes[node].d);
+        const int split = d.x, meta = d.y, last = d.z;
+        Box2T<DIM> lb, rb;
+        unpack_child<DIM>(ls, lb);
+        unpack_child<DIM>(rs, rb);
+        const bool lact = ((meta >> 8) & 0xff) != 0, ract = ((meta >> 16) & 0xff) != 0;
+        bool lok = split > qw && (qact || lact);
+        bool rok = last > qw && (qact || ract);
+        if (lok && (meta & kMetaLeftLeaf)) { leaf(split, lb); lok = false; }
+        if (rok && (meta & kMetaRightLeaf)) { leaf(split + 1, rb); rok = false; }
+        lok = lok && boxes_may_intersect<DIM>(qbox, lb);
+        rok = rok && boxes_may_intersect<DIM>(qbox, rb);
+        if (lok) {
+            if (rok) {
+                if (sp < kStackDepth) stack[sp++][tid] = split + 1;
+                else atomicOr(&cnt->err, kErrStack);
+            }
+            node = split;
+        } else if (rok) {
+            node = split + 1;
+        } else if (sp == 0) {
+            done = true;
+        } else {
+            node = stack[--sp][tid];
+        }
+    }
+    flush(true);
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(128)
 k_traverse_packet(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
@@ -465,7 +598,9 @@ k_traverse_packet(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict
 // Stencil bits: VF a->b slot i = bit i, VF b->a slot i = bit 3+i,
 // EE (i,j) = bit 6 + 3i + j.
 // ---------------------------------------------------------------------------
-template <int DIM>
+// DISC = false: stencils only (the discrete test runs in k_discrete_pairs),
+// so the kernel keeps few registers and many warps in flight for its gathers.
+template <int DIM, bool DISC = true>
 __global__ void __launch_bounds__(256)
 k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, const int *__restrict__ P,
                const unsigned char *__restrict__ flags, const double *__restrict__ V1, int nv,
@@ -473,6 +608,7 @@ k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, cons
                int2 *__restrict__ disc, unsigned long long disc_cap, int continuous, int discrete, Counters *cnt,
                const unsigned long long *lo_ptr, const unsigned long long *hi_ptr)
 {
+    if constexpr (!DISC) discrete = 0;
     // pairs [lo, hi): the whole list, or one query chunk's part of it
     unsigned long long n = *(volatile const unsigned long long *)hi_ptr;
     if (n > pair_cap) n = pair_cap;
@@ -492,9 +628,9 @@ k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, cons
             if (continuous) bits = stencil_bits<DIM>(fa, fb, __ldg(flags + pr.x), __ldg(flags + pr.y));
         }
         if (continuous) {
-            const unsigned nvf = __popc(bits & 0x3fu), nee = __popc(bits >> 6);
-            unsigned long long bvf = warp_reserve(&cnt->n_vf, nvf);
-            unsigned long long bee = DIM == 3 ? warp_reserve(&cnt->n_ee, nee) : 0ull;
+            const unsigned nvf = __popc(bits & 0x3fu), nee = DIM == 3 ? __popc(bits >> 6) : 0u;
+            unsigned long long bvf, bee;
+            block_reserve2<256>(&cnt->n_vf, nvf, &cnt->n_ee, nee, bvf, bee);
             for (unsigned m = bits & 0x3fu; m; m &= m - 1) {
                 const int b = __ffs(m) - 1;
                 const int *vs = b < 3 ? fa : fb;
@@ -541,6 +677,66 @@ k_expand_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, cons
     }
 }
 
+// Discrete test of leaf pairs [lo, hi) alone (default_discrete_test,
+// BVHTree.cpp:464-500): the half of k_expand_pairs that gathers V1.
+template <int DIM>
+__global__ void __launch_bounds__(128)
+k_discrete_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, const int *__restrict__ P,
+                 const double *__restrict__ V1, int nv, int2 *__restrict__ disc, unsigned long long disc_cap,
+                 Counters *cnt, const unsigned long long *lo_ptr, const unsigned long long *hi_ptr)
+{
+    unsigned long long n = *(volatile const unsigned long long *)hi_ptr;
+    if (n > pair_cap) n = pair_cap;
+    unsigned long long lo = lo_ptr ? *(volatile const unsigned long long *)lo_ptr : 0ull;
+    if (lo > n) lo = n;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long idx = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+         idx += stride) {
+        const int2 pr = pairs[idx];
+        int fa[DIM], fb[DIM];
+        bool inb = true;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            fa[k] = __ldg(P + (size_t)pr.x * DIM + k);
+            fb[k] = __ldg(P + (size_t)pr.y * DIM + k);
+            inb = inb && fa[k] >= 0 && fa[k] < nv && fb[k] >= 0 && fb[k] < nv;
+        }
+        bool shared = false;
+#pragma unroll
+        for (int i = 0; i < DIM; ++i)
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) shared |= fa[i] == fb[j];
+        if (!inb) atomicOr(&cnt->err, kErrBadIndex);
+        if (shared || !inb) continue;
+        double A[DIM][DIM], B[DIM][DIM];
+#pragma unroll
+        for (int i = 0; i < DIM; ++i)
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                A[i][k] = __ldg(V1 + (size_t)fa[i] * DIM + k);
+                B[i][k] = __ldg(V1 + (size_t)fb[i] * DIM + k);
+            }
+        int hit;
+        if constexpr (DIM == 3) hit = tri_tri(A[0], A[1], A[2], B[0], B[1], B[2]);
+        else hit = seg_seg(A[0], A[1], B[0], B[1]);
+        if (hit) {
+            const unsigned long long slot = warp_append(&cnt->n_discrete);
+            if (slot < disc_cap) disc[slot] = pr;
+        }
+    }
+}
+
+void launch_discrete_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P, const double *V1,
+                           int nv, int2 *disc, unsigned long long disc_cap, Counters *cnt, int grid, cudaStream_t st,
+                           const unsigned long long *lo_ptr, const unsigned long long *hi_ptr)
+{
+    if (!hi_ptr) hi_ptr = &cnt->n_pairs;
+    if (dim == 3)
+        k_discrete_pairs<3><<<grid, 128, 0, st>>>(pairs, pair_cap, P, V1, nv, disc, disc_cap, cnt, lo_ptr, hi_ptr);
+    else
+        k_discrete_pairs<2><<<grid, 128, 0, st>>>(pairs, pair_cap, P, V1, nv, disc, disc_cap, cnt, lo_ptr, hi_ptr);
+}
+
 void launch_traverse_refill(int dim, int window, const Node *nodes, const void *leaf_box,
                             const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs,
                             unsigned long long cap, Counters *cnt, unsigned *cursor, cudaStream_t st, int q_begin,
@@ -572,6 +768,34 @@ void launch_traverse_refill(int dim, int window, const Node *nodes, const void *
         MCLCCD_REFILL_CASE(16)
     }
 #undef MCLCCD_REFILL_CASE
+}
+
+void launch_traverse_buffered(int dim, int window, const Node *nodes, const void *leaf_box,
+                              const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs,
+                              unsigned long long cap, Counters *cnt, cudaStream_t st, int q_begin, int q_end)
+{
+    if (n < 2) return;
+    if (q_end < 0 || q_end > n - 1) q_end = n - 1;
+    if (q_begin >= q_end) return;
+    const int g = (q_end - q_begin + 127) / 128;
+    const auto *lb3 = reinterpret_cast<const LeafBox<3> *>(leaf_box);
+    const auto *lb2 = reinterpret_cast<const LeafBox<2> *>(leaf_box);
+#define MCLCCD_BUF_CASE(Wv)                                                                                        \
+    case Wv:                                                                                                       \
+        if (dim == 3)                                                                                              \
+            k_traverse_window_buf<3, Wv><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, q_begin, q_end,     \
+                                                             pairs, cap, cnt);                                      \
+        else                                                                                                       \
+            k_traverse_window_buf<2, Wv><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, q_begin, q_end,     \
+                                                             pairs, cap, cnt);                                      \
+        return;
+    switch (window) {
+        MCLCCD_BUF_CASE(8)
+        MCLCCD_BUF_CASE(32)
+    default:
+        MCLCCD_BUF_CASE(16)
+    }
+#undef MCLCCD_BUF_CASE
 }
 
 void launch_traverse(int dim, int packet, int window, const Node *nodes, const void *leaf_box,
@@ -621,6 +845,15 @@ void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap
                          const unsigned long long *hi_ptr)
 {
     if (!hi_ptr) hi_ptr = &cnt->n_pairs;
+    if (!discrete) {   // stencils only: the lean instantiation
+        if (dim == 3)
+            k_expand_pairs<3, false><<<grid, 256, 0, st>>>(pairs, pair_cap, P, flags, V1, nv, vf, vf_cap, ee, ee_cap,
+                                                           disc, disc_cap, continuous, 0, cnt, lo_ptr, hi_ptr);
+        else
+            k_expand_pairs<2, false><<<grid, 256, 0, st>>>(pairs, pair_cap, P, flags, V1, nv, vf, vf_cap, ee, ee_cap,
+                                                           disc, disc_cap, continuous, 0, cnt, lo_ptr, hi_ptr);
+        return;
+    }
     if (dim == 3)
         k_expand_pairs<3><<<grid, 256, 0, st>>>(pairs, pair_cap, P, flags, V1, nv, vf, vf_cap, ee, ee_cap, disc,
                                                 disc_cap, continuous, discrete, cnt, lo_ptr, hi_ptr);

@@ -215,6 +215,28 @@ def device_results(t):
 
 @pytest.mark.parametrize("window", [8, 16, 32])
 @pytest.mark.parametrize("scene", ["wavy", "annulus", "active"])
+def test_walk_buffer_matches_window_walk(window, scene):
+    # the buffered walk (pairs collected per warp, written 32 at a time) finds
+    # the same leaf pairs as the window walk
+    V0, V1, F, eta = scenes.wavy_cloth(1025, rows=97, seed=5) if scene != "annulus" else scenes.annulus_2d(500, seed=6)
+    act = (np.arange(len(V0)) % 7 < 2).astype(np.int32) if scene == "active" else None
+    out = []
+    for buf in (0, 1):
+        t = BVHTree(V0.shape[1])
+        t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+        t.set_tuning(walk_window=window)
+        t.set_tuning(walk_buffer=buf)
+        t.update(V0, V1, F, active=act)
+        t.traverse(V0, V1, F)
+        out.append(device_results(t) + (t.counts()["leaf_pairs"],))
+    assert out[0][3] == out[1][3] > 0
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("window", [8, 16, 32])
+@pytest.mark.parametrize("scene", ["wavy", "annulus", "active"])
 def test_walk_refill_matches_window_walk(window, scene):
     # the refill walk (persistent warps, idle lanes refilled from a per-warp
     # query pool) finds the same leaf pairs as the window walk it reorders;
@@ -266,28 +288,66 @@ def test_fused_narrow_phase_against_port(port, scene):
     assert (c["vf"], c["ee"]) == (int(p["cand_is_vf"].sum()), int(len(p["cand_is_vf"]) - p["cand_is_vf"].sum()))
 
 
-def test_walk_refill_against_port(port):
+@pytest.mark.parametrize("form", ["walk_refill", "walk_buffer"])
+def test_walk_forms_against_port(port, form):
     V0, V1, F, eta = scenes.folded_cloth(40, seed=7)
     t = BVHTree(3)
     t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
-    t.set_tuning(walk_refill=1)
+    t.set_tuning(**{form: 1})
     t.update(V0, V1, F)
     t.traverse(V0, V1, F)
     check_against_port(t, port, V0, V1, F, eta)
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("dim", [3, 2])
-def test_rebinned_accd_against_port(port, dim):
-    # the re-binned ACCD form (heads and tails in separate warp passes) gives
-    # the same bits as the default one-stencil-per-thread form
+def test_rebinned_accd_against_port(port, dim, form):
+    # the re-binned ACCD forms (1: heads and tails in separate warp passes of
+    # one kernel; 2: a head kernel and a tail kernel over a queue of the
+    # stencils that go on) give the same bits as the one-stencil-per-thread form
     V0, V1, F, eta = scenes.folded_cloth(48, seed=21) if dim == 3 else scenes.annulus_2d(300, seed=22)
     t = BVHTree(dim)
     t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
-    t.set_tuning(accd_rebin=1)
+    t.set_tuning(accd_rebin=form)
     t.update(V0, V1, F)
     t.traverse(V0, V1, F)
-    assert t.get_tuning()["accd_rebin"] == 1
+    assert t.get_tuning()["accd_rebin"] == form
     check_against_port(t, port, V0, V1, F, eta)
+
+
+@pytest.mark.parametrize("scene", ["fold", "annulus"])
+def test_expand_split_against_port(port, scene):
+    # the stencil expansion and the discrete test as two kernels, with the
+    # split ACCD form: the reference's sets
+    V0, V1, F, eta = scenes.folded_cloth(40, seed=11) if scene == "fold" else scenes.annulus_2d(300, seed=12)
+    t = BVHTree(V0.shape[1])
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    t.set_tuning(expand_split=1, accd_rebin=2)
+    t.update(V0, V1, F)
+    t.traverse(V0, V1, F)
+    check_against_port(t, port, V0, V1, F, eta)
+
+
+def test_split_accd_full_size_step_equals_default():
+    # the split form on the 2.1M-triangle cloth, streamed per query chunk
+    # (the head kernel's queue is reset per chunk): the same hits and toi
+    torch = pytest.importorskip("torch")
+    V0, V1, F, eta = scenes.wavy_cloth(1025, rows=257, seed=2)
+    maps = []
+    for form in (0, 2):
+        t = BVHTree(3)
+        t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+        t.set_tuning(accd_rebin=form, expand_split=form // 2)
+        t.update(V0, V1, F)
+        t.traverse(V0, V1, F)
+        maps.append(hit_map(*t.hits()))
+        n = len(maps[-1])
+        hs = torch.empty((n + 64, 4), dtype=torch.int32).pin_memory()
+        hv = torch.empty(n + 64, dtype=torch.uint8).pin_memory()
+        ht = torch.empty(n + 64, dtype=torch.float64).pin_memory()
+        nh, _ = t.traverse_out(hs, hv, ht)
+        assert nh == n and hit_map(hs[:n].numpy(), hv[:n].numpy(), ht[:n].numpy()) == maps[-1]
+    assert maps[0] == maps[1] and len(maps[0]) > 1_000_000
 
 
 @pytest.mark.parametrize("scene", ["wavy129", "spheres", "annulus", "fold_big_motion"])
@@ -332,6 +392,40 @@ def test_refit_equals_rebuild(port):
     u = run_gpu(V0, V1b, F, eta, always_rebuild=True)
     for a, b in ((t.candidates(), u.candidates()),):
         assert np.array_equal(canonical_set(*a), canonical_set(*b))
+
+
+def test_quality_triggered_rebuild(port):
+    # F never changes while 12 spheres drift apart along their own random
+    # directions: every leaf box keeps its size, but the refit-only tree keeps
+    # the grouping of the first positions, so its internal boxes stretch over
+    # spheres now far apart; the quality trigger rebuilds it.  The results
+    # stay those of a freshly built tree.
+    V0, V1, F, eta = scenes.icospheres(12, 3, seed=5)
+    nvs = len(V0) // 12
+    vel = np.repeat(np.random.default_rng(6).normal(0.0, 0.15, (12, 3)), nvs, axis=0)
+    t = BVHTree(3)
+    t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+    X, Y = V0, V1
+    for step in range(8):
+        if step:
+            X, Y = X + vel, Y + vel
+        t.update(X, Y, F)
+        t.traverse(X, Y, F)
+        if step == 0:
+            check_against_port(t, port, X, Y, F, eta)
+    fresh = BVHTree(3)
+    fresh.options.box_eta = fresh.options.vf_ccd_eta = fresh.options.ee_ccd_eta = eta
+    fresh.update(X, Y, F)
+    fresh.traverse(X, Y, F)
+    assert np.array_equal(device_results(t)[0], device_results(fresh)[0])
+    assert device_results(t)[1] == device_results(fresh)[1]
+    builds, by_quality = t.build_stats()
+    assert by_quality >= 1 and builds == 1 + by_quality
+    t2 = BVHTree(3)
+    t2.set_tuning(rebuild_ratio=0)
+    t2.update(V0, V1, F)
+    t2.update(V0 + vel, V1 + vel, F)
+    assert t2.build_stats() == (1, 0)
 
 
 def test_options(port):
