@@ -570,6 +570,8 @@ def measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev):
         "stencils": int(c2["vf"] + c2["ee"])}
     del t2
 
+    out["certified_c2"] = measure_c2(args, stream, dev, ev)
+
     # differentiation form: 256 x 256 folded cloth, thickness 1e-3
     V0, V1, F, eta4 = scenes.folded_cloth(256)
     a0, a1, aF = (torch.from_numpy(x).to(dev) for x in (V0, V1, F))
@@ -597,6 +599,72 @@ def measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev):
     del t3
     if not args.no_batch:
         out["batch"] = measure_batch(args)
+    return out
+
+
+def measure_c2(args, stream, dev, ev, sample=10_000_000):
+    """Precision form on its own workload: 64 icospheres (subdivision 6,
+    5,242,880 tris; radii U[0.05, 0.1], centres in the unit cube, per-sphere
+    translation N(0, 0.05) plus N(0, 1e-3) per vertex), thickness 1e-3, in
+    FP64 and in the FP32-certified form: step and narrow-phase times, hits.
+    The toi of the certified form against FP64 on the first `sample`
+    candidates of the FP64 tree and on the 100k constructed stress stencils
+    (near-parallel EE, near-coplanar VF), through the bulk call in both
+    precisions: hit/miss agreement, toi never later, relative error."""
+    import ctypes
+    import torch
+    from mclccd_b200 import MEM_DEVICE, PREC_FP32_CERTIFIED, PREC_FP64, BVHTree, narrow_phase_bulk, scenes
+    V0, V1, F, eta = scenes.icospheres(64, 6, seed=0)
+    d0, d1, dF = (torch.from_numpy(x).to(dev) for x in (V0, V1, F))
+    out = {"workload": f"64 icospheres, subdivision 6 ({len(F)} tris), thickness 1e-3, seed 0"}
+    cs = cv = None
+    for name, prec in (("fp64", PREC_FP64), ("fp32cert", PREC_FP32_CERTIFIED)):
+        t = BVHTree(3, precision=prec)
+        t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
+        t.options.profile = True
+        t.set_stream(stream.cuda_stream)
+        t.update(d0, d1, dF)
+        t.traverse()
+        ms, nar = [], []
+        for _ in range(3):
+            a, b = ev(), ev()
+            a.record(stream)
+            t.update(d0, d1, dF)
+            t.traverse()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+            nar.append(t.stage_ms()["narrow"])
+        c = t.counts()
+        ps = t.precision_stats()
+        out[name] = {"step_ms": float(np.median(ms)), "narrow_ms": float(np.median(nar)), "hits": int(c["hits"]),
+                     "stencils": int(c["vf"] + c["ee"]), "leaf_pairs": int(c["leaf_pairs"]),
+                     "fp64_pass_stencils": int(ps[0]), "toi_bound_hits": int(ps[1])}
+        if prec == PREC_FP64:   # a prefix of the candidate list, on the device
+            k = min(sample, int(c["vf"] + c["ee"]))
+            cs = torch.empty((k, 4), dtype=torch.int32, device=dev)
+            cv = torch.empty(k, dtype=torch.uint8, device=dev)
+            t._L.mclccd_get_candidates(t._h, MEM_DEVICE, k, ctypes.c_void_p(cs.data_ptr()),
+                                       ctypes.c_void_p(cv.data_ptr()))
+        del t
+        torch.cuda.empty_cache()
+    out["narrow_speedup_fp32cert_vs_fp64"] = out["fp64"]["narrow_ms"] / out["fp32cert"]["narrow_ms"]
+    out["same_hit_count"] = out["fp64"]["hits"] == out["fp32cert"]["hits"]
+
+    def compare(a0, a1, s4, kind, e):
+        t64, h64 = narrow_phase_bulk(a0, a1, s4, kind, e, precision=PREC_FP64)
+        tc, hc, nfb = narrow_phase_bulk(a0, a1, s4, kind, e, precision=PREC_FP32_CERTIFIED, return_fallbacks=True)
+        if not torch.is_tensor(t64):
+            t64, h64, tc, hc = (torch.from_numpy(x) for x in (t64, h64, tc, hc))
+        hit = h64 == 1
+        rel = torch.where(hit & (t64 > 0), (t64 - tc) / t64, torch.zeros_like(t64))
+        return {"stencils": int(len(h64)), "hits": int(hit.sum()), "hit_miss_identical": bool((h64 == hc).all()),
+                "later_than_fp64": int((hit & (tc > t64)).sum()), "max_rel_toi_error": float(rel.abs().max()),
+                "exact_toi": int((hit & (tc == t64)).sum()), "fp64_fallbacks": int(nfb)}
+
+    out["sample"] = compare(d0, d1, cs, cv, eta)
+    sV0, sV1, ssten, svf, seta = scenes.stress_stencils(100_000)
+    out["stress"] = compare(sV0, sV1, ssten, svf, seta)
     return out
 
 

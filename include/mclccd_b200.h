@@ -388,14 +388,21 @@ int mclccd_stage_ms(const mclccd_tree *tree, float *ms, int n);
  * done from a per-warp pool of queries, so lanes do not idle behind the
  * longest walk of their warp; window 8, 16 or 32; 0: one query per thread
  * start to end), the expansion split (1: the stencil expansion and the
- * discrete test as two kernels; 0: one kernel), and the rebuild ratio (in
- * percent; default 150): every refit sums the box areas of the internal
- * nodes relative to those of the leaves, and when that grows past the ratio
+ * discrete test as two kernels; 2: the same with the discrete test's lanes
+ * compacted, each warp queueing the pairs that share no vertex in shared
+ * memory and testing them 32 at a time; 0: one kernel), and the rebuild ratio (in
+ * percent; default 150): after each build and every fourth refit the box
+ * areas of the internal nodes are summed relative to those of the leaves,
+ * and when that grows past the ratio
  * of its value after the last full build, the next update rebuilds the
  * hierarchy (0: refit whenever P is unchanged), and the buffered walk (1:
  * the window walk collects each warp's leaf pairs in shared memory and
- * writes them 32 at a time with one atomic; window 8, 16 or 32).  Results do
- * not depend on any of them. */
+ * writes them in runs of 32 with one atomic, which also keeps neighbouring
+ * queries' pairs together for the kernels that read them; 2, the default:
+ * runs of 64; 0: one atomic per leaf test that hits; windows 0, 64 and 128
+ * take the unbuffered walk).
+ * The expansion split is on by default as well.  Results do not depend on
+ * any of them. */
 #define MCLCCD_TUNE_EXPAND_GRID 0
 #define MCLCCD_TUNE_ACCD_GRID 1
 #define MCLCCD_TUNE_WALK_PACKET 2

@@ -237,7 +237,8 @@ class BVHTree:
 
     def set_tuning(self, **kv):
         """Launch-shape knobs (expand_grid, accd_grid, walk_packet, accd_rebin, walk_window, overlap,
-        narrow_fused, fused_grid, walk_refill, expand_split, rebuild_ratio, walk_buffer); results never depend on them."""
+        narrow_fused, fused_grid, walk_refill, expand_split, rebuild_ratio, walk_buffer); results
+        never depend on them."""
         for k, v in kv.items():
             self._check(self._L.mclccd_set_tuning(self._h, self.TUNE_KEYS[k], int(v)), self._h)
 

@@ -27,6 +27,8 @@ constexpr int kAccdGrid = 148 * 128;
 // The fused pairs -> ACCD kernel is grid-stride over warp batches: one wave
 // of resident blocks (6 per SM).
 constexpr int kFusedGrid = 148 * 6;
+// the tree-quality sum runs after every full build and every 4th refit
+constexpr int kQualityEvery = 4;
 constexpr int kMaxAttempts = 6;
 
 struct DeviceGuard {
@@ -72,7 +74,7 @@ struct mclccd_tree {
     double *h_quality = nullptr;         // pinned copy of the two sums
     double q_build = 0.0;                // tree quality (internal / leaf box areas) after the last build
     bool force_rebuild = false;          // the refit-only tree degraded: rebuild at the next update
-    long long n_builds = 0, n_quality_rebuilds = 0;
+    long long n_builds = 0, n_quality_rebuilds = 0, refits_since_check = 0;
     DevBuf tq_idx, tq_state, tq_count;   // continuing-stencil queue of the split ACCD form
     std::vector<DevBuf *> all()
     {
@@ -95,7 +97,7 @@ struct mclccd_tree {
     cudaEvent_t out_ev[16] = {};
     unsigned long long *h_snap = nullptr;
     unsigned long long out_done = 0;   // hits already copied out by the streamed path
-    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0, 0, kFusedGrid, 0, 0, 150, 0};
+    int tune[MCLCCD_TUNE_COUNT] = {kExpandGrid, kAccdGrid, 0, 0, 16, 0, 0, kFusedGrid, 0, 1, 150, 2};
     // The fused narrow phase counts the candidate lists without writing them;
     // mclccd_get_candidates rebuilds them from the leaf pairs and the P of the
     // last traverse.
@@ -172,8 +174,10 @@ static int launch_walk(mclccd_tree *t, int dim, int packet, int np, Counters *cn
                                np, as<int2>(t->pairs), t->cap_pairs, cnt, as<unsigned>(t->walk_cursor), st, qb, qe);
         return MCLCCD_OK;
     }
-    if (!packet && t->tune[MCLCCD_TUNE_WALK_BUFFER]) {
-        launch_traverse_buffered(dim, t->tune[MCLCCD_TUNE_WALK_WINDOW], as<Node>(t->nodes), t->leaf_box.p,
+    const int win = t->tune[MCLCCD_TUNE_WALK_WINDOW];
+    if (!packet && t->tune[MCLCCD_TUNE_WALK_BUFFER] && (win == 8 || win == 16 || win == 32)) {
+        launch_traverse_buffered(dim, t->tune[MCLCCD_TUNE_WALK_WINDOW], t->tune[MCLCCD_TUNE_WALK_BUFFER] >= 2 ? 64 : 32,
+                                 as<Node>(t->nodes), t->leaf_box.p,
                                  as<unsigned char>(t->leaf_active), as<int>(t->vals), np, as<int2>(t->pairs),
                                  t->cap_pairs, cnt, st, qb, qe);
         return MCLCCD_OK;
@@ -689,9 +693,10 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
     MC_CUDA(t, ensure(t->leaf_box, sizeof(double) * 4 * dim * (size_t)np));
     MC_CUDA(t, ensure(t->leaf_active, (size_t)np));
     MC_CUDA(t, ensure(t->visits, sizeof(int) * (size_t)std::max(1, np - 1)));
-    // tree quality: the refit also sums the box areas of its internal nodes
-    // and of its leaves
-    const bool track = np > 1 && t->tune[MCLCCD_TUNE_REBUILD_RATIO] > 0;
+    // tree quality: box areas of the internal nodes and of the leaves, summed
+    // after every build, then after every kQualityEvery-th refit
+    const bool track = np > 1 && t->tune[MCLCCD_TUNE_REBUILD_RATIO] > 0 &&
+                       (!same || ++t->refits_since_check % kQualityEvery == 0);
     launch_refit(dim, dV0, dV1, dP, np, pdim, nv, t->box_eta, dact, as<int>(t->vals), as<int>(t->leaf_parent),
                  as<Node>(t->nodes), as<int>(t->visits), t->leaf_box.p, as<unsigned char>(t->leaf_active), cnt, st);
     ++t->launches;
@@ -984,10 +989,14 @@ static int traverse_impl(mclccd_tree *t, const double *V0, const double *V1, int
         if (fused) {   // no candidate lists: only the hits need room
             need(r * (double)c.n_hits, t->cap_hits);
         } else {
+            // hits were counted over the stencils that fit their lists: scale
+            // by that shortfall too (the hit list is sized by its own count,
+            // not by the candidates, which can be many more)
+            const double done = (double)(std::min(c.n_vf, t->cap_vf) + std::min(c.n_ee, t->cap_ee));
+            const double rh = r * (done > 0 ? (double)(c.n_vf + c.n_ee) / done : 1.0);
             need(r * (double)c.n_vf, t->cap_vf);
             need(r * (double)c.n_ee, t->cap_ee);
-            // A hit is a candidate: this capacity never overflows on its own.
-            t->cap_hits = std::max(t->cap_hits, t->cap_vf + t->cap_ee);
+            need(rh * (double)c.n_hits, t->cap_hits);
         }
         if (!grow) break;
         // a retry regrows and rewrites the device lists: let copies of this
@@ -1463,9 +1472,12 @@ int mclccd_set_tuning(mclccd_tree *t, int key, int value)
 {
     if (!t || key < 0 || key >= MCLCCD_TUNE_COUNT) return MCLCCD_ERR_INVALID;
     const bool flag = key == MCLCCD_TUNE_WALK_PACKET || key == MCLCCD_TUNE_NARROW_FUSED ||
-                      key == MCLCCD_TUNE_WALK_REFILL || key == MCLCCD_TUNE_EXPAND_SPLIT ||
-                      key == MCLCCD_TUNE_WALK_BUFFER;
-    if (key == MCLCCD_TUNE_REBUILD_RATIO) {
+                      key == MCLCCD_TUNE_WALK_REFILL;
+    if (key == MCLCCD_TUNE_WALK_BUFFER) {
+        if (value < 0 || value > 2) return fail(t, MCLCCD_ERR_INVALID, "walk buffer must be 0, 1 or 2");
+    } else if (key == MCLCCD_TUNE_EXPAND_SPLIT) {
+        if (value < 0 || value > 2) return fail(t, MCLCCD_ERR_INVALID, "expansion split must be 0, 1 or 2");
+    } else if (key == MCLCCD_TUNE_REBUILD_RATIO) {
         if (value != 0 && (value < 101 || value > 100000))
             return fail(t, MCLCCD_ERR_INVALID, "rebuild ratio is 0 (never) or a percentage above 100");
     } else if (key == MCLCCD_TUNE_ACCD_REBIN) {
@@ -1475,11 +1487,11 @@ int mclccd_set_tuning(mclccd_tree *t, int key, int value)
     } else if (key == MCLCCD_TUNE_WALK_WINDOW) {
         if (value != 0 && value != 8 && value != 16 && value != 32 && value != 64 && value != 128)
             return fail(t, MCLCCD_ERR_INVALID, "walk window must be 0, 8, 16, 32, 64 or 128");
-        if ((t->tune[MCLCCD_TUNE_WALK_REFILL] || t->tune[MCLCCD_TUNE_WALK_BUFFER]) && (value == 0 || value > 32))
-            return fail(t, MCLCCD_ERR_INVALID, "the refill and buffered walks take a window of 8, 16 or 32");
-    } else if ((key == MCLCCD_TUNE_WALK_REFILL || key == MCLCCD_TUNE_WALK_BUFFER) && value == 1 &&
+        if (t->tune[MCLCCD_TUNE_WALK_REFILL] && (value == 0 || value > 32))
+            return fail(t, MCLCCD_ERR_INVALID, "the refill walk takes a window of 8, 16 or 32");
+    } else if (key == MCLCCD_TUNE_WALK_REFILL && value == 1 &&
                (t->tune[MCLCCD_TUNE_WALK_WINDOW] == 0 || t->tune[MCLCCD_TUNE_WALK_WINDOW] > 32)) {
-        return fail(t, MCLCCD_ERR_INVALID, "the refill and buffered walks take a window of 8, 16 or 32");
+        return fail(t, MCLCCD_ERR_INVALID, "the refill walk takes a window of 8, 16 or 32");
     } else if (flag ? (value != 0 && value != 1) : (value < 1 || value > (1 << 20)))
         return fail(t, MCLCCD_ERR_INVALID, "tuning value out of range");
     t->tune[key] = value;

@@ -45,14 +45,16 @@ void launch_expand_pairs(int dim, const int2 *pairs, unsigned long long pair_cap
                          int discrete, Counters *cnt, int grid, cudaStream_t st,
                          const unsigned long long *lo_ptr = nullptr, const unsigned long long *hi_ptr = nullptr);
 // the discrete test of leaf pairs [*lo, *hi) alone (hi == nullptr: the pair count)
-// the window walk with pairs collected per warp and written 32 at a time
-void launch_traverse_buffered(int dim, int window, const Node *nodes, const void *leaf_box,
+// the window walk with pairs collected per warp and written in runs of 32
+// (run < 64) or 64
+void launch_traverse_buffered(int dim, int window, int run, const Node *nodes, const void *leaf_box,
                               const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs,
                               unsigned long long cap, Counters *cnt, cudaStream_t st, int q_begin = 0,
                               int q_end = -1);
 void launch_discrete_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P, const double *V1,
                            int nv, int2 *disc, unsigned long long disc_cap, Counters *cnt, int grid, cudaStream_t st,
-                           const unsigned long long *lo_ptr = nullptr, const unsigned long long *hi_ptr = nullptr);
+                           const unsigned long long *lo_ptr = nullptr, const unsigned long long *hi_ptr = nullptr,
+                           bool compact = false);
 void launch_snapshot(const unsigned long long *a, unsigned long long *da, const unsigned long long *b,
                      unsigned long long *db, cudaStream_t st);
 

@@ -385,7 +385,10 @@ k_traverse_refill(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict
 // pair counter, instead of one atomic per leaf test that hits.  The warp's
 // loops run in step (a lane that is done idles until the whole warp is), so
 // every flush is a whole-warp operation.
-template <int DIM, int W>
+// RUN: pairs are written in whole runs of RUN (32 or 64), which keeps the
+// pairs of neighbouring queries together in the list for the kernels that
+// read it.
+template <int DIM, int W, int RUN = 32>
 __global__ void __launch_bounds__(128, 4)
 k_traverse_window_buf(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
                       const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
@@ -393,7 +396,7 @@ k_traverse_window_buf(const Node *__restrict__ nodes, const LeafBox<DIM> *__rest
 {
     constexpr int S = DIM == 3 ? 3 : 2;
     constexpr int NB = 127 + W;
-    constexpr int OUT = 96;   // < 32 left after a flush + at most 64 per step
+    constexpr int OUT = RUN + 64;   // < RUN left after a flush + at most 64 per step
     __shared__ float s_box[NB][4 * DIM];
     __shared__ unsigned char s_act[NB];
     __shared__ int stack[kStackDepth][128];
@@ -430,7 +433,7 @@ k_traverse_window_buf(const Node *__restrict__ nodes, const LeafBox<DIM> *__rest
     auto flush = [&](bool all) {
         __syncwarp();
         const int c = s_nout[w];
-        const int take = all ? c : (c & ~31);
+        const int take = all ? c : (c / RUN) * RUN;
         if (take == 0) return;
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(&cnt->n_pairs, (unsigned long long)take);
@@ -438,8 +441,8 @@ k_traverse_window_buf(const Node *__restrict__ nodes, const LeafBox<DIM> *__rest
         for (int i = lane; i < take; i += 32)
             if (base + i < cap) pairs[base + i] = s_out[w][i];
         __syncwarp();
-        const int rest = c - take;   // < 32 <= take: source and destination do not overlap
-        if (lane < rest) s_out[w][lane] = s_out[w][take + lane];
+        const int rest = c - take;   // < RUN <= take: source and destination do not overlap
+        for (int i = lane; i < rest; i += 32) s_out[w][i] = s_out[w][take + i];
         __syncwarp();
         if (lane == 0) s_nout[w] = rest;
         __syncwarp();
@@ -726,11 +729,105 @@ k_discrete_pairs(const int2 *__restrict__ pairs, unsigned long long pair_cap, co
     }
 }
 
+// The same test with the lanes compacted: each warp reads 32 pairs per step,
+// drops those that share a vertex (most leaf pairs of a mesh are neighbours)
+// and queues the rest in shared memory; whenever 32 are queued the whole warp
+// runs the test on them, so the V1 gathers and the test run on full warps.
+template <int DIM>
+__global__ void __launch_bounds__(128)
+k_discrete_pairs_compact(const int2 *__restrict__ pairs, unsigned long long pair_cap, const int *__restrict__ P,
+                         const double *__restrict__ V1, int nv, int2 *__restrict__ disc, unsigned long long disc_cap,
+                         Counters *cnt, const unsigned long long *lo_ptr, const unsigned long long *hi_ptr)
+{
+    __shared__ int2 s_pr[4][64];
+    __shared__ int s_v[4][64][2 * DIM];
+    unsigned long long n = *(volatile const unsigned long long *)hi_ptr;
+    if (n > pair_cap) n = pair_cap;
+    unsigned long long lo = lo_ptr ? *(volatile const unsigned long long *)lo_ptr : 0ull;
+    if (lo > n) lo = n;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    auto test = [&](int slot) {
+        double A[DIM][DIM], B[DIM][DIM];
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) {
+            const int a = s_v[w][slot][i], b = s_v[w][slot][DIM + i];
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                A[i][k] = __ldg(V1 + (size_t)a * DIM + k);
+                B[i][k] = __ldg(V1 + (size_t)b * DIM + k);
+            }
+        }
+        int hit;
+        if constexpr (DIM == 3) hit = tri_tri(A[0], A[1], A[2], B[0], B[1], B[2]);
+        else hit = seg_seg(A[0], A[1], B[0], B[1]);
+        if (hit) {
+            const unsigned long long slot_out = warp_append(&cnt->n_discrete);
+            if (slot_out < disc_cap) disc[slot_out] = s_pr[w][slot];
+        }
+    };
+    int queued = 0;   // warp-uniform
+    const unsigned long long wstride = (unsigned long long)gridDim.x * 4 * 32;
+    for (unsigned long long base = lo + ((unsigned long long)blockIdx.x * 4 + w) * 32; base < n; base += wstride) {
+        const unsigned long long idx = base + lane;
+        bool keep = idx < n;
+        int2 pr = make_int2(0, 0);
+        int fa[DIM], fb[DIM];
+        if (keep) {
+            pr = pairs[idx];
+            bool inb = true;
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                fa[k] = __ldg(P + (size_t)pr.x * DIM + k);
+                fb[k] = __ldg(P + (size_t)pr.y * DIM + k);
+                inb = inb && fa[k] >= 0 && fa[k] < nv && fb[k] >= 0 && fb[k] < nv;
+            }
+            bool shared = false;
+#pragma unroll
+            for (int i = 0; i < DIM; ++i)
+#pragma unroll
+                for (int j = 0; j < DIM; ++j) shared |= fa[i] == fb[j];
+            if (!inb) atomicOr(&cnt->err, kErrBadIndex);
+            keep = inb && !shared;
+        }
+        const unsigned m = __ballot_sync(full, keep);
+        if (keep) {
+            const int pos = queued + __popc(m & lanemask_lt());   // < 31 + 32 = 63
+            s_pr[w][pos] = pr;
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) { s_v[w][pos][k] = fa[k]; s_v[w][pos][DIM + k] = fb[k]; }
+        }
+        queued += __popc(m);
+        __syncwarp();
+        if (queued >= 32) {
+            test(lane);
+            __syncwarp();
+            queued -= 32;   // move entries 32 .. 32 + queued - 1 to the front
+            if (lane < queued) {
+                s_pr[w][lane] = s_pr[w][32 + lane];
+#pragma unroll
+                for (int k = 0; k < 2 * DIM; ++k) s_v[w][lane][k] = s_v[w][32 + lane][k];
+            }
+            __syncwarp();
+        }
+    }
+    if (lane < queued) test(lane);
+}
+
 void launch_discrete_pairs(int dim, const int2 *pairs, unsigned long long pair_cap, const int *P, const double *V1,
                            int nv, int2 *disc, unsigned long long disc_cap, Counters *cnt, int grid, cudaStream_t st,
-                           const unsigned long long *lo_ptr, const unsigned long long *hi_ptr)
+                           const unsigned long long *lo_ptr, const unsigned long long *hi_ptr, bool compact)
 {
     if (!hi_ptr) hi_ptr = &cnt->n_pairs;
+    if (compact) {
+        if (dim == 3)
+            k_discrete_pairs_compact<3><<<grid, 128, 0, st>>>(pairs, pair_cap, P, V1, nv, disc, disc_cap, cnt, lo_ptr,
+                                                              hi_ptr);
+        else
+            k_discrete_pairs_compact<2><<<grid, 128, 0, st>>>(pairs, pair_cap, P, V1, nv, disc, disc_cap, cnt, lo_ptr,
+                                                              hi_ptr);
+        return;
+    }
     if (dim == 3)
         k_discrete_pairs<3><<<grid, 128, 0, st>>>(pairs, pair_cap, P, V1, nv, disc, disc_cap, cnt, lo_ptr, hi_ptr);
     else
@@ -770,7 +867,7 @@ void launch_traverse_refill(int dim, int window, const Node *nodes, const void *
 #undef MCLCCD_REFILL_CASE
 }
 
-void launch_traverse_buffered(int dim, int window, const Node *nodes, const void *leaf_box,
+void launch_traverse_buffered(int dim, int window, int run, const Node *nodes, const void *leaf_box,
                               const unsigned char *leaf_active, const int *sorted, int n, int2 *pairs,
                               unsigned long long cap, Counters *cnt, cudaStream_t st, int q_begin, int q_end)
 {
@@ -782,12 +879,20 @@ void launch_traverse_buffered(int dim, int window, const Node *nodes, const void
     const auto *lb2 = reinterpret_cast<const LeafBox<2> *>(leaf_box);
 #define MCLCCD_BUF_CASE(Wv)                                                                                        \
     case Wv:                                                                                                       \
-        if (dim == 3)                                                                                              \
+        if (run >= 64) {                                                                                           \
+            if (dim == 3)                                                                                          \
+                k_traverse_window_buf<3, Wv, 64><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, q_begin,    \
+                                                                     q_end, pairs, cap, cnt);                       \
+            else                                                                                                   \
+                k_traverse_window_buf<2, Wv, 64><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, q_begin,    \
+                                                                     q_end, pairs, cap, cnt);                       \
+        } else if (dim == 3) {                                                                                     \
             k_traverse_window_buf<3, Wv><<<g, 128, 0, st>>>(nodes, lb3, leaf_active, sorted, n, q_begin, q_end,     \
                                                              pairs, cap, cnt);                                      \
-        else                                                                                                       \
+        } else {                                                                                                   \
             k_traverse_window_buf<2, Wv><<<g, 128, 0, st>>>(nodes, lb2, leaf_active, sorted, n, q_begin, q_end,     \
                                                              pairs, cap, cnt);                                      \
+        }                                                                                                          \
         return;
     switch (window) {
         MCLCCD_BUF_CASE(8)

@@ -221,7 +221,7 @@ def test_walk_buffer_matches_window_walk(window, scene):
     V0, V1, F, eta = scenes.wavy_cloth(1025, rows=97, seed=5) if scene != "annulus" else scenes.annulus_2d(500, seed=6)
     act = (np.arange(len(V0)) % 7 < 2).astype(np.int32) if scene == "active" else None
     out = []
-    for buf in (0, 1):
+    for buf in (0, 1, 2):
         t = BVHTree(V0.shape[1])
         t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
         t.set_tuning(walk_window=window)
@@ -229,10 +229,11 @@ def test_walk_buffer_matches_window_walk(window, scene):
         t.update(V0, V1, F, active=act)
         t.traverse(V0, V1, F)
         out.append(device_results(t) + (t.counts()["leaf_pairs"],))
-    assert out[0][3] == out[1][3] > 0
-    assert np.array_equal(out[0][0], out[1][0])
-    assert out[0][1] == out[1][1]
-    assert np.array_equal(out[0][2], out[1][2])
+    for o in out[1:]:
+        assert out[0][3] == o[3] > 0
+        assert np.array_equal(out[0][0], o[0])
+        assert out[0][1] == o[1]
+        assert np.array_equal(out[0][2], o[2])
 
 
 @pytest.mark.parametrize("window", [8, 16, 32])
@@ -315,14 +316,16 @@ def test_rebinned_accd_against_port(port, dim, form):
     check_against_port(t, port, V0, V1, F, eta)
 
 
+@pytest.mark.parametrize("split", [1, 2])
 @pytest.mark.parametrize("scene", ["fold", "annulus"])
-def test_expand_split_against_port(port, scene):
-    # the stencil expansion and the discrete test as two kernels, with the
-    # split ACCD form: the reference's sets
+def test_expand_split_against_port(port, scene, split):
+    # the stencil expansion and the discrete test as two kernels (2: the
+    # discrete test on lane-compacted pairs), with the split ACCD form: the
+    # reference's sets
     V0, V1, F, eta = scenes.folded_cloth(40, seed=11) if scene == "fold" else scenes.annulus_2d(300, seed=12)
     t = BVHTree(V0.shape[1])
     t.options.box_eta = t.options.vf_ccd_eta = t.options.ee_ccd_eta = eta
-    t.set_tuning(expand_split=1, accd_rebin=2)
+    t.set_tuning(expand_split=split, accd_rebin=2)
     t.update(V0, V1, F)
     t.traverse(V0, V1, F)
     check_against_port(t, port, V0, V1, F, eta)
