@@ -28,6 +28,9 @@ namespace mclccd {
 #ifndef MCLCCD_WALK_MIN_BLOCKS
 #define MCLCCD_WALK_MIN_BLOCKS 5
 #endif
+#ifndef MCLCCD_WALK_BUF_MIN_BLOCKS
+#define MCLCCD_WALK_BUF_MIN_BLOCKS 4
+#endif
 constexpr int kStackDepth = MCLCCD_WALK_STACK;
 
 template <int DIM>
@@ -389,7 +392,7 @@ k_traverse_refill(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict
 // pairs of neighbouring queries together in the list for the kernels that
 // read it.
 template <int DIM, int W, int RUN = 32>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, MCLCCD_WALK_BUF_MIN_BLOCKS)
 k_traverse_window_buf(const Node *__restrict__ nodes, const LeafBox<DIM> *__restrict__ leaf_box,
                       const unsigned char *__restrict__ leaf_active, const int *__restrict__ sorted, int n,
                       int q_begin, int q_end, int2 *__restrict__ pairs, unsigned long long cap, Counters *cnt)
