@@ -242,11 +242,9 @@ __global__ void k_b_refit(const double *__restrict__ V0, const double *__restric
     bool right = __ldg(&nl[parent].d.x) != lk;
     write_child<DIM>(nl, parent, right, box, act);
     for (int level = 0; level < 256; ++level) {
-        __threadfence();
-        if (atomicAdd(vis + parent, 1) == 0) return;
-        __threadfence();
+        if (!refit_second_arrival(vis + parent)) return;
         const int node = parent;
-        merge_children<DIM>(nl + node, box, act);
+        merge_sibling<DIM>(nl + node, right, box, act);
         parent = __ldcg(&nl[node].d.w);
         if (parent < 0) return;
         const int psplit = __ldg(&nl[parent].d.x);

@@ -165,11 +165,9 @@ __global__ void k_refit(const double *__restrict__ V0, const double *__restrict_
     bool right = __ldg(&nodes[parent].d.x) != k;
     write_child<DIM>(nodes, parent, right, box, act);
     for (int level = 0; level < 256; ++level) {   // depth of a Karras tree over 30-bit keys is < 64
-        __threadfence();
-        if (atomicAdd(visits + parent, 1) == 0) return;   // sibling subtree not done yet
-        __threadfence();
+        if (!refit_second_arrival(visits + parent)) return;   // sibling subtree not done yet
         const int node = parent;
-        merge_children<DIM>(nodes + node, box, act);
+        merge_sibling<DIM>(nodes + node, right, box, act);
         parent = __ldcg(&nodes[node].d.w);
         if (parent < 0) return;   // root: its own box is never needed
         const int psplit = __ldg(&nodes[parent].d.x);

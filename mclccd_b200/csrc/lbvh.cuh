@@ -66,22 +66,34 @@ __device__ __forceinline__ void write_child(Node *nodes, int parent, bool right,
     reinterpret_cast<unsigned char *>(&nd->d.y)[right ? 2 : 1] = act ? 1 : 0;
 }
 
+// Refit arrival at a node: one acquire-release add on its visit counter.  The
+// first child's thread releases its box (written to the node before the add)
+// and stops; the second acquires that box and climbs on.
+__device__ __forceinline__ bool refit_second_arrival(int *counter)
+{
+    int prev;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(prev) : "l"(counter) : "memory");
+    return prev != 0;
+}
+
+// The second child to arrive at a node during the refit: merge the sibling's
+// box (written by the first) into this child's box and activity.
 template <int DIM>
-__device__ __forceinline__ void merge_children(const Node *nd, Box2T<DIM> &out, bool &act)
+__device__ __forceinline__ void merge_sibling(const Node *nd, bool right, Box2T<DIM> &box, bool &act)
 {
     constexpr int S = DIM == 3 ? 3 : 2;
-    float4 ls[S], rs[S];
+    float4 ss[S];
+    const float4 *src = right ? nd->l : nd->r;
 #pragma unroll
-    for (int i = 0; i < S; ++i) { ls[i] = __ldcg(&nd->l[i]); rs[i] = __ldcg(&nd->r[i]); }
+    for (int i = 0; i < S; ++i) ss[i] = __ldcg(src + i);
     const int meta = __ldcg(&nd->d.y);
-    act = ((meta >> 8) & 0xff) || ((meta >> 16) & 0xff);
-    Box2T<DIM> a, b;
-    unpack_child<DIM>(ls, a);
-    unpack_child<DIM>(rs, b);
+    act = act || ((meta >> (right ? 8 : 16)) & 0xff);
+    Box2T<DIM> b;
+    unpack_child<DIM>(ss, b);
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
-        out.t0lo[k] = fminf(a.t0lo[k], b.t0lo[k]); out.t0hi[k] = fmaxf(a.t0hi[k], b.t0hi[k]);
-        out.t1lo[k] = fminf(a.t1lo[k], b.t1lo[k]); out.t1hi[k] = fmaxf(a.t1hi[k], b.t1hi[k]);
+        box.t0lo[k] = fminf(box.t0lo[k], b.t0lo[k]); box.t0hi[k] = fmaxf(box.t0hi[k], b.t0hi[k]);
+        box.t1lo[k] = fminf(box.t1lo[k], b.t1lo[k]); box.t1hi[k] = fmaxf(box.t1hi[k], b.t1hi[k]);
     }
 }
 
