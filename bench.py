@@ -489,7 +489,7 @@ def measure_dropin(args, V0, V1a, V1b, F, eta, c):
     exe_dir = tempfile.mkdtemp(prefix="mclccd_dropin_")
     try:
         exe = os.path.join(exe_dir, "dropin_bench")
-        subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+        subprocess.run(["g++", "-std=c++17", "-O2", "-pthread", "-I", os.path.join(ROOT, "include"),
                         os.path.join(ROOT, "tests", "cpp", "dropin_bench.cpp"), "-L", os.path.join(ROOT, "mclccd_b200"),
                         "-lmclccd_b200", "-Wl,-rpath," + os.path.join(ROOT, "mclccd_b200"), "-o", exe], check=True)
         scene = os.path.join(exe_dir, "scene.bin")
@@ -513,7 +513,9 @@ def measure_dropin(args, V0, V1a, V1b, F, eta, c):
             "d2h_bytes_per_step": int(r["hits"] * (16 + 1 + 8) + r["discrete"] * 8),
             "hits_delivered": r["hits"], "discrete_delivered": r["discrete"],
             "api": "C++ mcl::BVHTree<double,3>: update(V0,V1,F,nf,3) + traverse(V0,V1,F) on host arrays, "
-                   "append_pair / append_discrete called for every result (wall clock)"}
+                   "append_pair / append_discrete called for every result (wall clock); options.threaded on, as "
+                   "in the reference, so append_pair runs on all host threads (thread-local counting hook)",
+            "host_threads": os.cpu_count()}
 
 
 def measure_forms(args, tree, stage, dV0, V1s, dF, eta, flush, stream, dev, ev):

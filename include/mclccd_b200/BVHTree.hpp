@@ -7,13 +7,20 @@
 //
 // Same members as the reference: Options (same fields and defaults),
 // update(), traverse(), and the hooks append_pair, append_discrete,
-// filter_pair and narrow_phase.  After traverse() the hooks are called from
-// the calling thread, fed from the device result buffers:
+// filter_pair and narrow_phase.  After traverse() the hooks are called on the
+// host, fed from the device result buffers:
 //   * append_pair(sten, is_vf, toi) once per CCD hit (toi >= 0);
 //   * append_discrete(p0, p1) once per discrete pair until it returns true;
 //   * filter_pair / narrow_phase, when set, are applied on the host to the
 //     candidate stencils (the default device ACCD scores the survivors when
 //     only filter_pair is set).
+// With options.threaded (the default, as in the reference, whose TBB
+// traversal calls these hooks from its worker threads) append_pair,
+// filter_pair and narrow_phase are called from several host threads at once,
+// so they must be thread-safe, as the reference requires; an exception
+// thrown by one is rethrown by traverse().  With threaded = false every hook
+// runs on the calling thread, in order.  append_discrete always runs on the
+// calling thread, so that returning true stops the dispatch exactly.
 // EE stencils and discrete pairs come with the lower primitive index first.
 // Errors throw mcl::CCDError (the reference asserts or silently returns).
 //
@@ -33,8 +40,11 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <exception>
 #include <limits>
 #include <memory>
+#include <mutex>
+#include <thread>
 #include <type_traits>
 #include <functional>
 #include <stdexcept>
@@ -481,9 +491,40 @@ private:
             t = static_cast<double *>(out_t_.p);
             check(mclccd_get_hits(h_, MCLCCD_MEM_HOST, nh, s, v, t));
         }
-        for (long long i = 0; i < nh; ++i) append_pair(make_stencil(&s[4 * i]), v[i] != 0, to_toi(t[i]));
+        for_each_result(nh, [&](long long i) { append_pair(make_stencil(&s[4 * i]), v[i] != 0, to_toi(t[i])); });
         dispatch_discrete();
         return true;
+    }
+    // f(i) for i in [0, n): on the calling thread, or with options.threaded
+    // over the host's hardware threads in contiguous slices (results of at
+    // least kMinPerThread per thread).  The first exception a slice throws is
+    // rethrown here after every slice has stopped.
+    static constexpr long long kMinPerThread = 1 << 15;
+    template <class F>
+    void for_each_result(long long n, F &&f) const
+    {
+        const long long hw = std::max<long long>(1, (long long)std::thread::hardware_concurrency());
+        const long long nt = options.threaded ? std::min(hw, n / kMinPerThread) : 1;
+        if (nt <= 1) {
+            for (long long i = 0; i < n; ++i) f(i);
+            return;
+        }
+        std::exception_ptr err;
+        std::mutex err_m;
+        auto slice = [&](long long k) {
+            try {
+                for (long long i = n * k / nt, e = n * (k + 1) / nt; i < e; ++i) f(i);
+            } catch (...) {
+                std::lock_guard<std::mutex> g(err_m);
+                if (!err) err = std::current_exception();
+            }
+        };
+        std::vector<std::thread> th;
+        th.reserve((size_t)nt - 1);
+        for (long long k = 1; k < nt; ++k) th.emplace_back(slice, k);
+        slice(0);
+        for (auto &x : th) x.join();
+        if (err) std::rethrow_exception(err);
     }
     void dispatch_discrete()
     {
@@ -545,16 +586,23 @@ private:
             std::vector<int> cs;
             std::vector<unsigned char> cv;
             candidates(cs, cv);
+            std::vector<unsigned char> skip(cv.size(), 0);
+            if (filter_pair)
+                for_each_result((long long)cv.size(), [&](long long i) {
+                    skip[i] = filter_pair(make_stencil(&cs[4 * i]), cv[i] != 0) ? 1 : 0;
+                });
             std::vector<int> ks;
             std::vector<unsigned char> kv;
             for (size_t i = 0; i < cv.size(); ++i) {
-                if (filter_pair && filter_pair(make_stencil(&cs[4 * i]), cv[i] != 0)) continue;
+                if (skip[i]) continue;
                 ks.insert(ks.end(), cs.begin() + 4 * i, cs.begin() + 4 * i + 4);
                 kv.push_back(cv[i]);
             }
             std::vector<double> toi(kv.size(), -1.0);
             if (narrow_phase) {
-                for (size_t i = 0; i < kv.size(); ++i) toi[i] = narrow_phase(make_stencil(&ks[4 * i]), kv[i] != 0);
+                for_each_result((long long)kv.size(), [&](long long i) {
+                    toi[i] = narrow_phase(make_stencil(&ks[4 * i]), kv[i] != 0);
+                });
             } else if (!kv.empty()) {
                 if (!V0 || mem_ != MCLCCD_MEM_HOST)
                     throw CCDError(MCLCCD_ERR_INVALID, "filter_pair without narrow_phase needs host V0/V1 at traverse");
@@ -577,14 +625,17 @@ private:
                                                   nullptr));
             }
             if (append_pair)
-                for (size_t i = 0; i < kv.size(); ++i)
+                for_each_result((long long)kv.size(), [&](long long i) {
                     if (toi[i] >= 0) append_pair(make_stencil(&ks[4 * i]), kv[i] != 0, to_toi(toi[i]));
+                });
         } else if (append_pair) {
             std::vector<int> s;
             std::vector<unsigned char> v;
             std::vector<double> t;
             hits(s, v, t);
-            for (size_t i = 0; i < v.size(); ++i) append_pair(make_stencil(&s[4 * i]), v[i] != 0, to_toi(t[i]));
+            for_each_result((long long)v.size(), [&](long long i) {
+                append_pair(make_stencil(&s[4 * i]), v[i] != 0, to_toi(t[i]));
+            });
         }
         dispatch_discrete();
     }

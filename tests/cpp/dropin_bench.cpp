@@ -8,12 +8,37 @@
 //   dropin_bench scene.bin warmup steps
 // scene.bin: int32 nv, nf; f64 eta; nv x 3 f64 V0, V1a, V1b; nf x 3 int32 F.
 // Prints one JSON object: per-step ms, hits and discrete pairs delivered.
+// options.threaded is on (the reference's default), so append_pair runs on
+// several host threads; the hook counts into thread-local accumulators that
+// each dispatch thread adds to the totals when it ends.
 #include "mclccd_b200/BVHTree.hpp"
 
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 #include <vector>
+
+namespace {
+std::mutex g_m;
+long long g_hits = 0;
+double g_toi = 0;
+struct Acc {
+    long long hits = 0;
+    double toi = 0;
+    void flush()
+    {
+        std::lock_guard<std::mutex> g(g_m);
+        g_hits += hits;
+        g_toi += toi;
+        hits = 0;
+        toi = 0;
+    }
+    ~Acc() { flush(); }
+};
+thread_local Acc t_acc;
+} // namespace
 
 int main(int argc, char **argv)
 {
@@ -36,7 +61,10 @@ int main(int argc, char **argv)
     tree.options.box_eta = tree.options.vf_ccd_eta = tree.options.ee_ccd_eta = eta;
     long long hits = 0, disc = 0;
     double toi_sum = 0;
-    tree.append_pair = [&](const mcl::Stencil &, bool, const double &toi) { ++hits; toi_sum += toi; };
+    tree.append_pair = [](const mcl::Stencil &, bool, const double &toi) {
+        ++t_acc.hits;
+        t_acc.toi += toi;
+    };
     tree.append_discrete = [&](int, int) -> bool { ++disc; return false; };
     tree.update(V0.data(), V1a.data(), F.data(), nf, 3);   // first update: full build, untimed
     const double *V1s[2] = {V1b.data(), V1a.data()};
@@ -44,11 +72,16 @@ int main(int argc, char **argv)
     long long last_hits = 0, last_disc = 0;
     for (int i = 0; i < warmup + steps; ++i) {
         const double *V1 = V1s[i % 2];
-        hits = disc = 0;
+        disc = 0;
+        g_hits = 0;
+        g_toi = 0;
         const auto t0 = std::chrono::steady_clock::now();
         tree.update(V0.data(), V1, F.data(), nf, 3);
         tree.traverse(V0.data(), V1, F.data());
+        t_acc.flush();   // this thread's share (the others flushed as they ended)
         const auto t1 = std::chrono::steady_clock::now();
+        hits = g_hits;
+        toi_sum = g_toi;
         if (i >= warmup) ms.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
         last_hits = hits;
         last_disc = disc;

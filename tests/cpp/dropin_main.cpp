@@ -3,11 +3,18 @@
 // append_discrete collecting into vectors.  Scene in, results out, as raw
 // little-endian binaries (written / read by tests/test_cpp_dropin.py).
 // A third argument "float" runs mcl::BVHTree<float, 3> on the coordinates
-// rounded to float (toi written widened to double).
+// rounded to float (toi written widened to double); "serial" sets
+// options.threaded = false (hooks on the calling thread, in order); "throw"
+// makes append_pair throw on its 100th call and exits 3 when traverse()
+// rethrows it.
 #include "mclccd_b200/BVHTree.hpp"
 
+#include <atomic>
 #include <cstdio>
 #include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
 #include <vector>
 
 template <typename T>
@@ -20,7 +27,9 @@ int run(const std::vector<double> &V0d, const std::vector<double> &V1d, const st
     std::vector<int> hs, ds;
     std::vector<double> ht;
     std::vector<unsigned char> hv;
+    std::mutex m;   // append_pair runs on several threads (options.threaded)
     tree.append_pair = [&](const mcl::Stencil &s, bool is_vf, const T &toi) {
+        std::lock_guard<std::mutex> g(m);
         for (int i = 0; i < 4; ++i) hs.push_back(s[i]);
         hv.push_back(is_vf ? 1 : 0);
         ht.push_back((double)toi);
@@ -61,14 +70,21 @@ int main(int argc, char **argv)
         std::fread(F.data(), 4, F.size(), f) != F.size())
         return 2;
     std::fclose(f);
-    if (argc == 4) return run<float>(V0, V1, F, np, eta, argv[2]);
+    const char *mode = argc == 4 ? argv[3] : "";
+    if (!std::strcmp(mode, "float")) return run<float>(V0, V1, F, np, eta, argv[2]);
+    const bool throws = !std::strcmp(mode, "throw");
 
     mcl::BVHTree<double, 3> tree;
     tree.options.box_eta = tree.options.vf_ccd_eta = tree.options.ee_ccd_eta = eta;
+    if (!std::strcmp(mode, "serial")) tree.options.threaded = false;
     std::vector<int> hs, ds;
     std::vector<double> ht;
     std::vector<unsigned char> hv;
+    std::mutex m;   // append_pair runs on several threads (options.threaded)
+    std::atomic<long long> calls(0);
     tree.append_pair = [&](const mcl::Stencil &s, bool is_vf, const double &toi) {
+        if (throws && calls.fetch_add(1) == 99) throw std::runtime_error("hook failed");
+        std::lock_guard<std::mutex> g(m);
         for (int i = 0; i < 4; ++i) hs.push_back(s[i]);
         hv.push_back(is_vf ? 1 : 0);
         ht.push_back(toi);
@@ -83,7 +99,11 @@ int main(int argc, char **argv)
     } catch (const mcl::CCDError &e) {
         std::fprintf(stderr, "CCDError %d: %s\n", e.status, e.what());
         return 1;
+    } catch (const std::runtime_error &e) {
+        std::fprintf(stderr, "hook exception: %s\n", e.what());
+        return 3;
     }
+    if (throws) return 4;   // the hook's exception was lost
     FILE *o = std::fopen(argv[2], "wb");
     int64_t n[2] = {(int64_t)hv.size(), (int64_t)ds.size() / 2};
     std::fwrite(n, 8, 2, o);

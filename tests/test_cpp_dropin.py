@@ -14,7 +14,7 @@ LIBDIR = os.path.join(ROOT, "mclccd_b200")
 
 def build_demo(tmp_path):
     exe = str(tmp_path / "dropin_main")
-    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), SRC,
+    subprocess.run(["g++", "-std=c++17", "-O2", "-pthread", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), SRC,
                     "-L", LIBDIR, "-lmclccd_b200", f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
     return exe
 
@@ -24,7 +24,10 @@ def test_dropin_header_compiles_and_links(tmp_path):
 
 
 @pytest.mark.gpu
-def test_dropin_hooks_match_oracle(tmp_path):
+@pytest.mark.parametrize("mode", ["threaded", "serial"])
+def test_dropin_hooks_match_oracle(tmp_path, mode):
+    # threaded: append_pair on all host threads (the reference's default);
+    # serial: options.threaded = false, on the calling thread
     from mclccd_b200 import scenes
     from oracle.ref import Port, canonical_set, sort_rows
     exe = build_demo(tmp_path)
@@ -35,7 +38,7 @@ def test_dropin_hooks_match_oracle(tmp_path):
         f.write(np.array([eta], np.float64).tobytes())
         f.write(V0.tobytes()); f.write(V1.tobytes()); f.write(F.astype(np.int32).tobytes())
     out = tmp_path / "out.bin"
-    subprocess.run([exe, str(scene), str(out)], check=True)
+    subprocess.run([exe, str(scene), str(out)] + (["serial"] if mode == "serial" else []), check=True)
     raw = out.read_bytes()
     nh, nd = np.frombuffer(raw[:16], np.int64)
     o = 16
@@ -49,6 +52,22 @@ def test_dropin_hooks_match_oracle(tmp_path):
     want = {(int(v),) + tuple(map(int, s)): float(t) for s, v, t in zip(p["hit_sten"], p["hit_is_vf"], p["hit_toi"])}
     assert got == want
     assert np.array_equal(sort_rows(ds), sort_rows(p["discrete"]))
+
+
+@pytest.mark.gpu
+def test_dropin_hook_exception_reaches_the_caller(tmp_path):
+    # an exception thrown by append_pair on a dispatch thread is rethrown by
+    # traverse() on the calling thread
+    from mclccd_b200 import scenes
+    exe = build_demo(tmp_path)
+    V0, V1, F, eta = scenes.folded_cloth(40, seed=21)
+    scene = tmp_path / "scene.bin"
+    with open(scene, "wb") as f:
+        f.write(np.array([len(V0), len(F), 3], np.int32).tobytes())
+        f.write(np.array([eta], np.float64).tobytes())
+        f.write(V0.tobytes()); f.write(V1.tobytes()); f.write(F.astype(np.int32).tobytes())
+    r = subprocess.run([exe, str(scene), str(tmp_path / "out.bin"), "throw"], capture_output=True, text=True)
+    assert r.returncode == 3 and "hook failed" in r.stderr, (r.returncode, r.stderr)
 
 
 @pytest.mark.gpu
@@ -105,7 +124,7 @@ def test_dropin_float_tree(tmp_path):
 
 def build_cpp(tmp_path, name):
     exe = str(tmp_path / name)
-    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
+    subprocess.run(["g++", "-std=c++17", "-O2", "-pthread", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
                     os.path.join(ROOT, "tests", "cpp", name + ".cpp"), "-L", LIBDIR, "-lmclccd_b200",
                     f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
     return exe
