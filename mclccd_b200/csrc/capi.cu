@@ -142,7 +142,6 @@ cudaError_t ensure(DevBuf &b, size_t bytes)
 
 template <typename T> T *as(DevBuf &b) { return reinterpret_cast<T *>(b.p); }
 
-cudaMemcpyKind h2d_or_d2d(int mem_kind) { return mem_kind == MCLCCD_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice; }
 
 int check_launch(mclccd_tree *t, const char *what)
 {
@@ -586,7 +585,26 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
     const bool prof = (t->flags & MCLCCD_OPT_PROFILE) != 0;
     if (prof) cudaEventRecord(t->ev[0], st);
     const long long pcount = (long long)np * pdim;
-    MC_CUDA(t, ensure(t->Pstage, sizeof(int) * (size_t)pcount));
+    const size_t pbytes = sizeof(int) * (size_t)pcount;
+    // The incoming P as the device reads it: the caller's device array as it
+    // is, or one copy of host P.  The handle's own copy (Pd) is rewritten
+    // only when the topology changed.
+    const bool dev_p = mem_kind == MCLCCD_MEM_DEVICE;
+    if (!dev_p) {
+        MC_CUDA(t, ensure(t->Pstage, pbytes));
+        MC_CUDA(t, cudaMemcpyAsync(t->Pstage.p, P, pbytes, cudaMemcpyHostToDevice, st));
+    }
+    const int *inP = dev_p ? P : as<int>(t->Pstage);
+    // Pd := the incoming P
+    auto adopt_p = [&]() -> cudaError_t {
+        if (!dev_p) {
+            std::swap(t->Pstage, t->Pd);
+            return cudaSuccess;
+        }
+        cudaError_t e = ensure(t->Pd, pbytes);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(t->Pd.p, P, pbytes, cudaMemcpyDeviceToDevice, st);
+        return e;
+    };
     // Refit-only when the topology is byte-identical to the previous update.
     const bool may_refit = t->built && t->np > 1 && !(t->flags & MCLCCD_OPT_ALWAYS_REBUILD) && np == t->np &&
                            pdim == t->pdim && !t->force_rebuild;
@@ -596,12 +614,11 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
         // The reference's update carries no vertex count: it is 1 + the
         // largest index in P, found on the device (with the refit check's
         // compare, one small read-back).
-        MC_CUDA(t, cudaMemcpyAsync(t->Pstage.p, P, sizeof(int) * (size_t)pcount, h2d_or_d2d(mem_kind), st));
         MC_CUDA(t, cudaMemsetAsync(t->diff.p, 0, 2 * sizeof(int), st));
-        launch_max_index(as<int>(t->Pstage), pcount, as<int>(t->diff) + 1, st);
+        launch_max_index(inP, pcount, as<int>(t->diff) + 1, st);
         ++t->launches;
         if (may_refit) {
-            launch_compare(as<int>(t->Pstage), as<int>(t->Pd), pcount, as<int>(t->diff), st);
+            launch_compare(inP, as<int>(t->Pd), pcount, as<int>(t->diff), st);
             ++t->launches;
         }
         MC_CUDA(t, cudaMemcpyAsync(t->h_diff, t->diff.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -627,23 +644,25 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
             dact = as<int>(t->actd);
         }
     }
-    if (!derive_nv)
-        MC_CUDA(t, cudaMemcpyAsync(t->Pstage.p, P, sizeof(int) * (size_t)pcount, h2d_or_d2d(mem_kind), st));
     MC_CUDA(t, cudaMemsetAsync(t->counters.p, 0, sizeof(Counters), st));
 
     bool same = may_refit && nv == t->nv;
+    // P still to be compared: the refit is launched before the answer is
+    // known (it runs while the host waits for the comparison alone), and a
+    // differing P adds the full build after it.
+    bool speculate = false;
     if (same && p_known >= 0) {
         same = p_known == 1;
     } else if (same) {
         MC_CUDA(t, cudaMemsetAsync(t->diff.p, 0, sizeof(int), st));
-        launch_compare(as<int>(t->Pstage), as<int>(t->Pd), pcount, as<int>(t->diff), st);
+        launch_compare(inP, as<int>(t->Pd), pcount, as<int>(t->diff), st);
         ++t->launches;
         MC_CUDA(t, cudaMemcpyAsync(t->h_diff, t->diff.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        MC_CUDA(t, cudaStreamSynchronize(st));
-        same = *t->h_diff == 0;
+        MC_CUDA(t, cudaEventRecord(t->ev[7], st));
+        speculate = true;
     }
-    std::swap(t->Pstage, t->Pd);
-    const int *dP = as<int>(t->Pd);
+    if (!speculate && !same) MC_CUDA(t, adopt_p());
+    const int *dP = as<int>(t->Pd);   // (reassigned when the comparison after a speculative refit fails)
     Counters *cnt = as<Counters>(t->counters);
 
     // Representative flags: recomputed only when the primitive count changes
@@ -671,6 +690,36 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
         t->flags_np = np;
     }
 
+    MC_CUDA(t, ensure(t->leaf_box, sizeof(double) * 4 * dim * (size_t)np));
+    MC_CUDA(t, ensure(t->leaf_active, (size_t)np));
+    MC_CUDA(t, ensure(t->visits, sizeof(int) * (size_t)std::max(1, np - 1)));
+    // the refit, with the tree-quality sum after every build and every
+    // kQualityEvery-th refit (box areas of the internal nodes and of the
+    // leaves)
+    bool track = false;
+    auto refit = [&](bool built) -> int {
+        track = np > 1 && t->tune[MCLCCD_TUNE_REBUILD_RATIO] > 0 &&
+                (built || ++t->refits_since_check % kQualityEvery == 0);
+        launch_refit(dim, dV0, dV1, dP, np, pdim, nv, t->box_eta, dact, as<int>(t->vals), as<int>(t->leaf_parent),
+                     as<Node>(t->nodes), as<int>(t->visits), t->leaf_box.p, as<unsigned char>(t->leaf_active), cnt, st);
+        ++t->launches;
+        if (track) {
+            MC_CUDA(t, ensure(t->quality, 2 * sizeof(double)));
+            launch_tree_quality(dim, as<Node>(t->nodes), np, as<double>(t->quality), st);
+            ++t->launches;
+        }
+        return check_launch(t, "refit kernel");
+    };
+    if (speculate) {
+        if (prof) cudaEventRecord(t->ev[1], st);
+        if (int rc = refit(false)) return rc;
+        MC_CUDA(t, cudaEventSynchronize(t->ev[7]));
+        same = *t->h_diff == 0;
+        if (!same) {
+            MC_CUDA(t, adopt_p());
+            dP = as<int>(t->Pd);
+        }
+    }
     if (!same) {
         MC_CUDA(t, ensure(t->cent, sizeof(float) * (size_t)np * dim));
         MC_CUDA(t, ensure(t->bounds, sizeof(unsigned) * 8));
@@ -689,23 +738,10 @@ int mclccd_update(mclccd_tree *t, const double *V0, const double *V1, int nv, co
         t->launches += 4 + 1 + sort_num_passes(30) + (np > 1 ? 1 : 0);
         if (int rc = check_launch(t, "build kernels")) return rc;
     }
-    if (prof) cudaEventRecord(t->ev[1], st);
-    MC_CUDA(t, ensure(t->leaf_box, sizeof(double) * 4 * dim * (size_t)np));
-    MC_CUDA(t, ensure(t->leaf_active, (size_t)np));
-    MC_CUDA(t, ensure(t->visits, sizeof(int) * (size_t)std::max(1, np - 1)));
-    // tree quality: box areas of the internal nodes and of the leaves, summed
-    // after every build, then after every kQualityEvery-th refit
-    const bool track = np > 1 && t->tune[MCLCCD_TUNE_REBUILD_RATIO] > 0 &&
-                       (!same || ++t->refits_since_check % kQualityEvery == 0);
-    launch_refit(dim, dV0, dV1, dP, np, pdim, nv, t->box_eta, dact, as<int>(t->vals), as<int>(t->leaf_parent),
-                 as<Node>(t->nodes), as<int>(t->visits), t->leaf_box.p, as<unsigned char>(t->leaf_active), cnt, st);
-    ++t->launches;
-    if (track) {
-        MC_CUDA(t, ensure(t->quality, 2 * sizeof(double)));
-        launch_tree_quality(dim, as<Node>(t->nodes), np, as<double>(t->quality), st);
-        ++t->launches;
+    if (!speculate || !same) {
+        if (prof && !speculate) cudaEventRecord(t->ev[1], st);
+        if (int rc = refit(!same)) return rc;
     }
-    if (int rc = check_launch(t, "refit kernel")) return rc;
     if (prof) cudaEventRecord(t->ev[2], st);
     MC_CUDA(t, cudaMemcpyAsync(t->h_cnt, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
     if (track)

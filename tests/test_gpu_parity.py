@@ -397,6 +397,33 @@ def test_refit_equals_rebuild(port):
         assert np.array_equal(canonical_set(*a), canonical_set(*b))
 
 
+def test_changed_topology_same_sizes_rebuilds(port):
+    # same np, pdim and nv but a different P: the refit launched before the
+    # comparison returns is followed by a full build, and the results are the
+    # new topology's.  (reptri off: with np unchanged the reference keeps the
+    # old representative flags, BVHTree.cpp:44-48, so only all-represented
+    # flags mean the same for both topologies.)
+    V0, V1, F, eta = scenes.wavy_cloth(97, seed=1)
+    t = run_gpu(V0, V1, F, eta, reptri=False)
+    assert t.build_stats()[0] == 1
+    G = np.ascontiguousarray(np.random.default_rng(5).permutation(F)[:, [1, 2, 0]])
+    p = port.run(V0, V1, G, eta, reptri=False)
+
+    def check():
+        assert np.array_equal(canonical_set(*t.candidates()), canonical_set(p["cand_sten"], p["cand_is_vf"]))
+        assert np.array_equal(sort_rows(t.discrete()), sort_rows(p["discrete"]))
+        assert hit_map(*t.hits()) == hit_map(p["hit_sten"], p["hit_is_vf"], p["hit_toi"])
+
+    t.update(V0, V1, G)
+    t.traverse(V0, V1, G)
+    assert t.build_stats()[0] == 2
+    check()
+    t.update(V0, V1, G)             # unchanged again: refit only
+    t.traverse(V0, V1, G)
+    assert t.build_stats()[0] == 2
+    check()
+
+
 def test_quality_triggered_rebuild(port):
     # F never changes while 12 spheres drift apart along their own random
     # directions: every leaf box keeps its size, but the refit-only tree keeps
