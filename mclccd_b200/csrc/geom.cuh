@@ -437,8 +437,16 @@ static __device__ __noinline__ int tt2_overlap(cpt p1, cpt q1_, cpt r1_, cpt p2,
 
 // Coplanar case: project on the axis plane maximising T1's area (normal n1);
 // for the x- and y-dominant planes the reference also exchanges p and q.
-static __device__ __noinline__ int tt3_coplanar(cpt p1, cpt q1, cpt r1, cpt p2, cpt q2, cpt r2, const double *n1)
+// The six vertices come by value (rows p1 q1 r1 p2 q2 r2), so the callers'
+// copies can stay in registers on the common path.
+struct TriPair {
+    double v[6][3];
+    double n[3];
+};
+static __device__ __noinline__ int tt3_coplanar(const TriPair t)
 {
+    const double *p1 = t.v[0], *q1 = t.v[1], *r1 = t.v[2], *p2 = t.v[3], *q2 = t.v[4], *r2 = t.v[5];
+    const double *n1 = t.n;
     const double nx = n1[0] < 0 ? -n1[0] : n1[0], ny = n1[1] < 0 ? -n1[1] : n1[1], nz = n1[2] < 0 ? -n1[2] : n1[2];
     int u, v;
     bool sw;
@@ -491,6 +499,25 @@ __device__ __forceinline__ bool tt3_canon(double dp, double dq, double dr, int &
     return true;
 }
 
+__device__ __forceinline__ TriPair tri_pair(cpt p1, cpt q1, cpt r1, cpt p2, cpt q2, cpt r2, cpt n)
+{
+    TriPair t;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        t.v[0][i] = p1[i]; t.v[1][i] = q1[i]; t.v[2][i] = r1[i];
+        t.v[3][i] = p2[i]; t.v[4][i] = q2[i]; t.v[5][i] = r2[i];
+        t.n[i] = n[i];
+    }
+    return t;
+}
+
+// o = (a, b, c)[k], by value, so the permuted vertices stay in registers.
+__device__ __forceinline__ void pick3(double (&o)[3], int k, const double *a, const double *b, const double *c)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) o[i] = k == 0 ? a[i] : (k == 1 ? b[i] : c[i]);
+}
+
 __device__ __forceinline__ int tri_tri(cpt p1, cpt q1, cpt r1, cpt p2, cpt q2, cpt r2)
 {
     double a[3], b[3], n1[3], n2[3];
@@ -507,20 +534,27 @@ __device__ __forceinline__ int tri_tri(cpt p1, cpt q1, cpt r1, cpt p2, cpt q2, c
 
     int rot1;
     bool sw2;
-    if (!tt3_canon(dp1, dq1, dr1, rot1, sw2)) return tt3_coplanar(p1, q1, r1, p2, q2, r2, n1);
-    cpt A1 = rot1 == 0 ? p1 : (rot1 == 1 ? q1 : r1);
-    cpt B1 = rot1 == 0 ? q1 : (rot1 == 1 ? r1 : p1);
-    cpt C1 = rot1 == 0 ? r1 : (rot1 == 1 ? p1 : q1);
-    cpt A2 = p2, B2 = sw2 ? r2 : q2, C2 = sw2 ? q2 : r2;
+    if (!tt3_canon(dp1, dq1, dr1, rot1, sw2)) return tt3_coplanar(tri_pair(p1, q1, r1, p2, q2, r2, n1));
+    // the permuted vertices are selected by value, not by pointer, so that
+    // they stay in registers (the same values reach the same operations)
+    double A1[3], B1[3], C1[3], B2[3], C2[3];
+    pick3(A1, rot1, p1, q1, r1);
+    pick3(B1, rot1, q1, r1, p1);
+    pick3(C1, rot1, r1, p1, q1);
+    pick3(B2, sw2 ? 1 : 0, q2, r2, r2);
+    pick3(C2, sw2 ? 1 : 0, r2, q2, q2);
     const double da = dp2, db = sw2 ? dr2 : dq2, dc = sw2 ? dq2 : dr2;
 
     int rot2;
     bool sw1;
-    if (!tt3_canon(da, db, dc, rot2, sw1)) return tt3_coplanar(A1, B1, C1, A2, B2, C2, n1);
-    cpt X2 = rot2 == 0 ? A2 : (rot2 == 1 ? B2 : C2);
-    cpt Y2 = rot2 == 0 ? B2 : (rot2 == 1 ? C2 : A2);
-    cpt Z2 = rot2 == 0 ? C2 : (rot2 == 1 ? A2 : B2);
-    return tt3_minmax(A1, sw1 ? C1 : B1, sw1 ? B1 : C1, X2, Y2, Z2);
+    if (!tt3_canon(da, db, dc, rot2, sw1)) return tt3_coplanar(tri_pair(A1, B1, C1, p2, B2, C2, n1));
+    double X2[3], Y2[3], Z2[3], M1[3], N1[3];
+    pick3(X2, rot2, p2, B2, C2);
+    pick3(Y2, rot2, B2, C2, p2);
+    pick3(Z2, rot2, C2, p2, B2);
+    pick3(M1, sw1 ? 1 : 0, B1, C1, C1);
+    pick3(N1, sw1 ? 1 : 0, C1, B1, B1);
+    return tt3_minmax(A1, M1, N1, X2, Y2, Z2);
 }
 
 // NarrowPhase<double,2>::discrete_edge_edge (NarrowPhase.cpp:229-257).
