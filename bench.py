@@ -173,19 +173,24 @@ def per_unit_figures():
 FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
-def fp64_roofline(c, narrow_ms, per=None):
+def fp64_roofline(c, narrow_ms, per=None, measured_tflops=None):
     """FP64 roofline of the narrow phase: the flops per VF and EE stencil
     counted on the oracle (the necessary work: add, multiply, divide and
     square root one flop each) times this run's stencils, over the narrow
-    stage's time."""
+    stage's time.  The peak is the FP64 FMA rate measured in this run
+    (mclccd_fp64_fma_rate) when given, else the nominal figure."""
     per = per_unit_figures() if per is None else per
     if "narrow_flops_per_vf" not in per or not narrow_ms or narrow_ms <= 0:
         return None
     flops = per["narrow_flops_per_vf"] * c["vf"] + per.get("narrow_flops_per_ee", 0.0) * c["ee"]
     achieved = flops / (narrow_ms / 1e3) / 1e12
-    return {"achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS,
-            "flops": flops, "peak_source": "nominal: 148 SMs x 64 FP64 FMA lanes x 2 flops x 1965 MHz "
-                                           "(no measured FP64 peak exists for this pool)",
+    if measured_tflops:
+        peak, src = measured_tflops, ("measured in this run: FP64 FMA throughput of this GPU "
+                                      "(mclccd_fp64_fma_rate, 8 independent FMA chains per thread)")
+    else:
+        peak, src = FP64_PEAK_TFLOPS, "nominal: 148 SMs x 64 FP64 FMA lanes x 2 flops x 1965 MHz"
+    return {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "flops": flops,
+            "peak_source": src, "peak_nominal": FP64_PEAK_TFLOPS, "frac_of_nominal": achieved / FP64_PEAK_TFLOPS,
             "flops_source": "oracle/count_flops.py: necessary FP64 operations per stencil, per kind "
                             "(profiles/narrow_flops_per_stencil.txt)"}
 
@@ -385,7 +390,12 @@ def run_b200(args, rank, world, local):
     top = max(kt, key=kt.get)
     peak, src = measured_peaks()
     tr = measured_traffic(c, fused)
-    fp = fp64_roofline(c, kt["narrow"])
+    try:
+        from mclccd_b200.ccd import fp64_fma_rate
+        fp64_measured = fp64_fma_rate(dev.index or 0)
+    except Exception:
+        fp64_measured = None
+    fp = fp64_roofline(c, kt["narrow"], measured_tflops=fp64_measured)
     hbm = {k: {"ms": kt[k], "algorithmic_bytes": ab[k],
                "GB/s": ab[k] / (kt[k] / 1e3) / 1e9 if kt[k] > 0 else None,
                "frac": ab[k] / (kt[k] / 1e3) / 1e9 / peak if kt[k] > 0 else None,

@@ -422,6 +422,12 @@ int mclccd_get_tuning(const mclccd_tree *tree, int key, int *value);
 /* Kernels launched by this handle since creation (for launch accounting). */
 int mclccd_kernel_launches(const mclccd_tree *tree, long long *n);
 
+/* Measured FP64 fused multiply-add throughput of a device, in TFLOP/s (one
+ * FMA = 2 flops): eight independent FMA chains per thread over one wave of
+ * 8 x 256-thread blocks per SM.  A diagnostic with no counterpart in the
+ * reference: the measured denominator of the FP64 narrow phase's roofline. */
+int mclccd_fp64_fma_rate(int device, double *tflops);
+
 /* Human-readable message of the handle's last failure ("" if none). */
 const char *mclccd_last_error(const mclccd_tree *tree);
 const char *mclccd_status_string(int status);

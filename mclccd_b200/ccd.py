@@ -87,6 +87,7 @@ def lib():
         "mclccd_get_tuning": ([vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mclccd_kernel_launches": ([vp, llp], C.c_int),
         "mclccd_build_stats": ([vp, llp, llp], C.c_int),
+        "mclccd_fp64_fma_rate": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
         "mclccd_last_error": ([vp], C.c_char_p),
         "mclccd_status_string": ([C.c_int], C.c_char_p),
     }
@@ -96,6 +97,16 @@ def lib():
         f.restype = res
     _lib = L
     return L
+
+
+def fp64_fma_rate(device: int = 0) -> float:
+    """Measured FP64 FMA throughput of a device in TFLOP/s
+    (mclccd_fp64_fma_rate)."""
+    out = C.c_double(0.0)
+    rc = lib().mclccd_fp64_fma_rate(device, C.byref(out))
+    if rc != 0:
+        raise CCDError(rc, "mclccd_fp64_fma_rate failed")
+    return out.value
 
 
 def _is_torch_cuda(a) -> bool:

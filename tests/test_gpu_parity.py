@@ -596,3 +596,11 @@ def test_float32_coordinates():
             t.update(a0, a1, aF)   # refit-only second step, traverse on the update's arrays
             t.traverse()
             assert hit_map(*t.hits()) == want
+
+
+def test_fp64_fma_rate_is_a_b200_figure():
+    # the measured denominator of the narrow phase's FP64 roofline: below the
+    # nominal 148 SMs x 64 lanes x 2 flops x 1.965 GHz and well above zero
+    from mclccd_b200.ccd import fp64_fma_rate
+    r = fp64_fma_rate(0)
+    assert 5.0 < r <= 148 * 64 * 2 * 1.965e9 / 1e12 * 1.02, r
