@@ -61,6 +61,10 @@ def test_fp64_roofline_of_the_narrow_phase():
     assert abs(r["achieved"] - want) < 1e-9 and r["unit"] == "TFLOP/s"
     assert abs(r["peak"] - 37.22) < 0.01 and abs(r["frac"] - want / r["peak"]) < 1e-12
     assert bench.fp64_roofline(c, 0.0, per) is None and bench.fp64_roofline(c, 1.0, {}) is None
+    # with the FP64 FMA rate measured in the run, that is the denominator
+    m = bench.fp64_roofline(c, 1.0, per, measured_tflops=34.0)
+    assert m["peak"] == 34.0 and abs(m["frac"] - want / 34.0) < 1e-12 and m["peak_source"].startswith("measured")
+    assert abs(m["frac_of_nominal"] - r["frac"]) < 1e-12
 
 
 def test_committed_flops_match_the_oracle_count():
