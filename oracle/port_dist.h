@@ -10,6 +10,13 @@
 #ifndef MCLCCD_ORACLE_PORT_DIST_H
 #define MCLCCD_ORACLE_PORT_DIST_H
 
+/* PORT_BRANCH(id) marks the case a routine takes (oracle/dist_err.cpp records
+ * it to compare the case taken in FP64 and in higher precision); empty
+ * otherwise. */
+#ifndef PORT_BRANCH
+#define PORT_BRANCH(id)
+#endif
+
 /* ---------------------------------------------------------------------- */
 /* Distances.                                                                */
 /* ---------------------------------------------------------------------- */
@@ -31,20 +38,21 @@ double port_vf_distance3(const double *pt, const double *p1, const double *p2, c
     if (s + t < det) {
         if (s < 0) {
             if (t < 0) {
-                if (d < 0) { s = clamp_zero_one(-d / a); t = 0; }
-                else { s = 0; t = clamp_zero_one(-e / c); }
-            } else { s = 0; t = clamp_zero_one(-e / c); }
-        } else if (t < 0) { s = clamp_zero_one(-d / a); t = 0; }
-        else { double inv = 1.0 / det; s *= inv; t *= inv; }
+                if (d < 0) { PORT_BRANCH(1); s = clamp_zero_one(-d / a); t = 0; }
+                else { PORT_BRANCH(2); s = 0; t = clamp_zero_one(-e / c); }
+            } else { PORT_BRANCH(3); s = 0; t = clamp_zero_one(-e / c); }
+        } else if (t < 0) { PORT_BRANCH(4); s = clamp_zero_one(-d / a); t = 0; }
+        else { PORT_BRANCH(5); double inv = 1.0 / det; s *= inv; t *= inv; }
     } else {
         if (s < 0) {
             double t0 = b + d, t1 = c + e;
-            if (t1 > t0) { double num = t1 - t0, den = a - 2.0 * b + c; s = clamp_zero_one(num / den); t = 1 - s; }
-            else { t = clamp_zero_one(-e / c); s = 0; }
+            if (t1 > t0) { PORT_BRANCH(6); double num = t1 - t0, den = a - 2.0 * b + c; s = clamp_zero_one(num / den); t = 1 - s; }
+            else { PORT_BRANCH(7); t = clamp_zero_one(-e / c); s = 0; }
         } else if (t < 0) {
-            if (a + d > b + e) { double num = c + e - b - d, den = a - 2.0 * b + c; s = clamp_zero_one(num / den); t = 1 - s; }
-            else { s = clamp_zero_one(-e / c); t = 0; }
+            if (a + d > b + e) { PORT_BRANCH(8); double num = c + e - b - d, den = a - 2.0 * b + c; s = clamp_zero_one(num / den); t = 1 - s; }
+            else { PORT_BRANCH(9); s = clamp_zero_one(-e / c); t = 0; }
         } else {
+            PORT_BRANCH(10);
             double num = c + e - b - d, den = a - 2.0 * b + c;
             s = clamp_zero_one(num / den); t = 1 - s;
         }
@@ -66,9 +74,9 @@ double port_ee_distance3(const double *p0, const double *p1, const double *q0, c
     if (denom != 0) s = clamp01((b * f - c * e) / denom);
     else s = 0;
     double tnom = b * s + f;
-    if (tnom < 0 || e == 0) { t = 0; s = (a == 0) ? 0 : clamp01(-c / a); }
-    else if (tnom > e) { t = 1.0; s = (a == 0) ? 0 : clamp01((b - c) / a); }
-    else t = tnom / e;
+    if (tnom < 0 || e == 0) { PORT_BRANCH(denom != 0 ? 11 : 21); t = 0; s = (a == 0) ? 0 : clamp01(-c / a); }
+    else if (tnom > e) { PORT_BRANCH(denom != 0 ? 12 : 22); t = 1.0; s = (a == 0) ? 0 : clamp01((b - c) / a); }
+    else { PORT_BRANCH(denom != 0 ? 13 : 23); t = tnom / e; }
     double w[3];
     for (int k = 0; k < 3; ++k) w[k] = (q0[k] + t * d2[k]) - (p0[k] + s * d1[k]);
     return sqrt(dot3(w, w));
