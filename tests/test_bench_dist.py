@@ -89,3 +89,25 @@ def test_algorithmic_bytes_forms():
     assert fused["expand"] == 0 and fused["walk"] == lists["walk"] and fused["refit"] == lists["refit"]
     # the fused form neither writes nor reads the 16 B stencil records
     assert fused["narrow"] == lists["expand"] + lists["narrow"] - 2 * 16 * (c["vf"] + c["ee"])
+
+
+def test_reference_arm_line_on_a_small_cloth():
+    # the reference arm's JSON line (the reference's own code on the host's
+    # cores, same metric, unit and direction as the device arm): a 65 x 65
+    # cloth keeps it to seconds
+    import json
+    import subprocess
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libmclccd_ref.so")):
+        import pytest
+        pytest.skip("reference oracle not built")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "65",
+                          "--steps", "2", "--warmup", "1"], capture_output=True, text=True, check=True,
+                         cwd=ROOT).stdout
+    line = json.loads([x for x in out.splitlines() if x.startswith("{")][-1])
+    assert line["impl"] == "reference" and line["unit"] == "stencils/s" and line["higher_is_better"] is True
+    assert line["steps"] == 2 and line["warmup"] == 1 and line["value"] > 0
+    assert line["config"]["tris"] == 2 * 64 * 64 and line["config"]["stencils_per_step"] > 0
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
