@@ -29,6 +29,11 @@ constexpr int kAccdGrid = 148 * 128;
 constexpr int kFusedGrid = 148 * 6;
 // the tree-quality sum runs after every full build and every 4th refit
 constexpr int kQualityEvery = 4;
+// The discrete test is grid-stride over the leaf pairs (128-thread blocks).
+#ifndef MCLCCD_DISCRETE_GRID
+#define MCLCCD_DISCRETE_GRID (148 * 128)
+#endif
+constexpr int kDiscreteGrid = MCLCCD_DISCRETE_GRID;
 constexpr int kMaxAttempts = 6;
 
 struct DeviceGuard {
@@ -199,7 +204,7 @@ static int launch_expand(mclccd_tree *t, int dim, const int *dP, const double *d
                             as<int4>(t->vf), t->cap_vf, as<int4>(t->ee), t->cap_ee, as<int2>(t->disc), t->cap_disc,
                             cont, 0, cnt, t->tune[MCLCCD_TUNE_EXPAND_GRID], st, lo, hi);
         launch_discrete_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, dV1, nv, as<int2>(t->disc), t->cap_disc, cnt,
-                              148 * 16, st, lo, hi);
+                              kDiscreteGrid, st, lo, hi, t->tune[MCLCCD_TUNE_EXPAND_SPLIT] == 2);
         return 2;
     }
     launch_expand_pairs(dim, as<int2>(t->pairs), t->cap_pairs, dP, as<unsigned char>(t->pflags), dV1, nv,
